@@ -1,0 +1,181 @@
+/*
+ * massccs_gpu.h -- C-ABI of the B200 trajectory engine (libmassccs_gpu.so).
+ *
+ * The drop-in boundary for the reference's trajectory loop.  In the reference
+ * (cces-cepid/massccs) the hot path is the body of the OpenMP loop in
+ * System::System (src/System.cpp:204-285): per trajectory, System::setup
+ * (src/System.cpp:1397-1518), then run_He / run_N2 / run_CO2
+ * (src/System.cpp:338-1392), which call the Force::*_LC routines
+ * (src/Force.cpp:34-1725) over the LinkedCell tables (src/LinkedCell.cpp:19-440).
+ * The reference has no FFI of its own; these entry points are what a host that
+ * keeps the reference's set-up (Input, MoleculeTarget, ellipsoid, RNG pre-draw)
+ * and its reduction (src/System.cpp:287-321) binds in place of that loop.
+ *
+ * Conventions
+ *  - Plain C types only; every function returns a ccs_status (0 = success).
+ *  - The host owns every input and output array; the library copies them and
+ *    owns all device memory of a context.
+ *  - One host thread per context; calls on one context are serialised.
+ *  - No exceptions cross the ABI; ccs_last_error() describes the last failure.
+ *  - Units are the reference's: Angstrom, fs, amu, kcal/mol, e.
+ */
+#ifndef MASSCCS_GPU_H
+#define MASSCCS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCS_ABI_VERSION 1
+
+typedef enum {
+  CCS_OK = 0,
+  CCS_ERR_INVALID = -1,     /* bad argument or call order */
+  CCS_ERR_NOMEM = -2,       /* host or device allocation failed */
+  CCS_ERR_CUDA = -3,        /* CUDA runtime error (message in ccs_last_error) */
+  CCS_ERR_TIMEOUT = -4,     /* the device watchdog stopped the kernel */
+  CCS_ERR_NODEVICE = -5,    /* no usable CUDA device / not built for it */
+  CCS_ERR_UNSUPPORTED = -6  /* a configuration this engine does not implement */
+} ccs_status;
+
+/* Buffer gases, numbered as Input.cpp:134-150 (gas_buffer_flag). */
+typedef enum {
+  CCS_GAS_HE = 1,   /* 1 site */
+  CCS_GAS_N2 = 2,   /* 2 N + massless central charge (GasBuffer.cpp:79-115) */
+  CCS_GAS_CO2 = 3,  /* O-C-O, Harris-Yung (GasBuffer.cpp:116-165) */
+  CCS_GAS_AR = 4,   /* 1 site */
+  CCS_GAS_CO2_1SITE = 5 /* "co2": 1 site (GasBuffer.cpp:178-190) */
+} ccs_gas;
+
+typedef enum {
+  CCS_PREC_FP32 = 0, /* forces and integration in FP32; 1-cos(chi) in FP64 */
+  CCS_PREC_FP64 = 1  /* everything in FP64 (the oracle-matching mode) */
+} ccs_precision;
+
+/* Trajectory status, as the reference classifies trajectories (System.cpp:217-227). */
+typedef enum {
+  CCS_TRAJ_FREE = 0,    /* missed the ellipsoid: counted, dOmega = 0 */
+  CCS_TRAJ_SCATTER = 1, /* left the ellipsoid/box within the energy tolerance */
+  CCS_TRAJ_LOST = 2,    /* ran out of retries: excluded from the denominator */
+  CCS_TRAJ_CAPPED = 3   /* hit the per-try step cap (the reference would not end) */
+} ccs_traj_status;
+
+/* quirks bits */
+#define CCS_QUIRK_CO2_VCM 1 /* reproduce System.cpp:1012 (vcm[0] = gasProbe->vcm[1]) */
+
+/* Run parameters: the scalars System passes to setup/run_* and Force
+ * (System.h:57-100, Force.cpp:20-26), plus engine knobs.  Fill with
+ * ccs_params_default() first. */
+typedef struct {
+  int32_t gas;              /* ccs_gas */
+  int32_t force_type;       /* 1..6, System.cpp:49-87 */
+  double dt;                /* fs */
+  double temperature;       /* K */
+  double mu;                /* amu: reduced mass (atomic gases) or gas mass (N2, CO2) */
+  double gas_inertia;       /* amu A^2, sum m z^2 of the gas sites (System.cpp:109-112) */
+  double d_bond;            /* A, constrained pair distance (GasBuffer d) */
+  double alpha;             /* polarizability already in kcal/mol units (System.cpp:117) */
+  double lj_cutoff;         /* A */
+  double coul_cutoff;       /* A */
+  double skin;              /* A, the reference cell edge is lj_cutoff + skin */
+  double a, b, c;           /* ellipsoid semi-axes, A */
+  double bmax;              /* maximal impact parameter, A */
+  double lx, ly, lz;        /* half box lengths (System.cpp:142-144), A */
+  int32_t precision;        /* ccs_precision */
+  int32_t quirks;           /* CCS_QUIRK_* bits */
+  double cell_size;         /* engine cell edge in A; 0 = automatic */
+  int32_t lanes_per_traj;   /* 0 = autotuned, else 1,2,4,8,16 or 32 lanes per trajectory */
+  int32_t block_size;       /* 0 = automatic (multiple of 32) */
+  uint32_t max_steps_per_try; /* 0 = 2,000,000 */
+  double watchdog_s;        /* kernel wall-time budget, 0 = 600 s */
+} ccs_params;
+
+/* Per-run statistics. */
+typedef struct {
+  uint64_t ntraj, nfree, nscatter, nlost, ncapped;
+  uint64_t steps;           /* integration steps, all tries */
+  uint64_t visits;          /* site x atom pairs the engine evaluated */
+  uint64_t force_calls;     /* site force evaluations */
+  double kernel_ms;         /* device time of the trajectory kernel (CUDA events) */
+  double h2d_ms, d2h_ms;    /* copy times of ccs_run (CUDA events) */
+  int32_t lanes_per_traj, block_size, grid_size, reserved;
+} ccs_stats;
+
+typedef struct ccs_ctx ccs_ctx;
+
+/* Library version and the ABI it implements. */
+int ccs_version(int32_t *abi_version);
+
+/* Create a context on a CUDA device (replaces the per-trajectory `new Force` /
+ * `new GasBuffer` of System.cpp:211-213 with one long-lived device context). */
+int ccs_create(ccs_ctx **out, int device);
+void ccs_destroy(ccs_ctx *ctx);
+
+/* Defaults for every field of ccs_params (He, force_type 4, reference defaults). */
+void ccs_params_default(ccs_params *p);
+
+/* Target atoms (MoleculeTarget arrays, MoleculeTarget.h:74-92, in the
+ * reference's oriented frame).  eps/sig are the pair parameters for the
+ * probe's LJ sites exactly as MoleculeTarget::assignedParameter produces them
+ * (MoleculeTarget.cpp:540-570); eps_c/sig_c the CO2 carbon-site parameters
+ * (NULL unless gas = CO2).  The library builds its own cell grid from them
+ * (LinkedCell.cpp:19-440 is the reference counterpart).  Call ccs_set_params
+ * first: the grid depends on the cutoffs and force type. */
+int ccs_set_target(ccs_ctx *ctx, size_t natoms, const double *x, const double *y, const double *z,
+                   const double *q, const double *eps, const double *sig, const double *eps_c,
+                   const double *sig_c);
+
+/* Scalar parameters (System.cpp:19-144 results).  Resets the target grid. */
+int ccs_set_params(ccs_ctx *ctx, const ccs_params *p);
+
+/* Run ntraj trajectories (System.cpp:204-285).  rnd[k] are the reference's
+ * pre-drawn arrays rnd_vec1..9 (System.cpp:184-197): rnd[0] = sqrt(bmax^2 u1),
+ * rnd[1..4] = u2..u5, rnd[5..8] = u6..u9 (only read for N2/CO2, may be NULL
+ * otherwise).  Outputs (host arrays of ntraj; steps/visits may be NULL):
+ * status (ccs_traj_status), one_minus_cos = 1 - cos(chi) for scatter else 0,
+ * steps = integration steps over all tries, visits = engine pair visits.
+ * Synchronous. */
+int ccs_run(ccs_ctx *ctx, size_t ntraj, const double *const rnd[9], int8_t *status,
+            double *one_minus_cos, uint32_t *steps, uint32_t *visits, ccs_stats *stats);
+
+/* Same on device buffers, asynchronous on `stream` (a cudaStream_t, NULL =
+ * the context's stream).  d_rnd holds 9 rows of `stride` doubles.  Statistics
+ * are accumulated on the device and read back by ccs_sync_stats. */
+int ccs_run_device(ccs_ctx *ctx, size_t ntraj, const double *d_rnd, size_t stride,
+                   int8_t *d_status, double *d_one_minus_cos, uint32_t *d_steps,
+                   uint32_t *d_visits, void *stream);
+int ccs_sync_stats(ccs_ctx *ctx, ccs_stats *stats);
+
+/* Force on gas site `site` at npts positions (pos: npts x 3), as the
+ * reference's per-site dispatch picks the routine (System.cpp:371-379,
+ * 594-637, 1028-1065 -> Force.cpp).  Same device code as the trajectory
+ * kernel.  Outputs: f (npts x 3), U (npts), visits (npts, may be NULL). */
+int ccs_eval_site_forces(ccs_ctx *ctx, size_t npts, int site, const double *pos, double *f,
+                         double *U, uint32_t *visits);
+
+/* Initial conditions of System::setup (System.cpp:1397-1518) for ntraj
+ * trajectories: hit flags and site positions/velocities (ntraj x 3 sites x 3). */
+int ccs_eval_setup(ccs_ctx *ctx, size_t ntraj, const double *const rnd[9], int8_t *hit,
+                   double *pos, double *vel);
+
+/* Engine description after ccs_set_target: grid and reach actually used. */
+typedef struct {
+  int32_t nx, ny, nz, natoms;
+  double cell_size, reach;
+  double origin[3];
+  int32_t charged, allpairs, max_cell_atoms, vel_table_len;
+  int32_t sm_count, reserved;
+} ccs_info;
+int ccs_get_info(ccs_ctx *ctx, ccs_info *info);
+
+/* Human-readable strings. */
+const char *ccs_status_string(int status);
+const char *ccs_last_error(ccs_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

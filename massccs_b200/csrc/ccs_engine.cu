@@ -1,0 +1,747 @@
+// ccs_engine.cu -- host side of libmassccs_gpu.so: the C-ABI of
+// include/massccs_gpu.h, the engine's cell grid, the speed-sampler table,
+// the launch autotuner and the kernel instantiations.
+//
+// Reference counterparts (cces-cepid/massccs):
+//   ccs_set_target  <- MoleculeTarget arrays + LinkedCell (src/LinkedCell.cpp:19-440)
+//   ccs_set_params  <- System members and Force ctor arguments (src/System.cpp:19-144,
+//                      src/Force.cpp:20-26)
+//   ccs_run         <- the OpenMP trajectory loop (src/System.cpp:204-285)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/massccs_gpu.h"
+#include "ccs_device.cuh"
+
+using namespace ccs;
+
+struct ccs_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[6] = {};
+  ccs_params p{};
+  bool have_params = false, have_target = false;
+  std::string err;
+  // engine grid
+  int nx = 0, ny = 0, nz = 0, natoms = 0, max_cell = 0;
+  double h = 0, origin[3] = {0, 0, 0}, bb_lo[3] = {0, 0, 0}, bb_hi[3] = {0, 0, 0}, reach = 0;
+  int charged = 0, allpairs = 0, coul_on = 0, dip_on = 0;
+  float4 *d_xyzq32 = nullptr;
+  float2 *d_ab32 = nullptr, *d_abc32 = nullptr;
+  double4 *d_xyzq64 = nullptr;
+  double2 *d_ab64 = nullptr, *d_abc64 = nullptr;
+  int *d_cell_start = nullptr;
+  // speed table
+  double *d_vtab_v = nullptr, *d_vtab_s = nullptr;
+  int vtab_n = 0;
+  // per-run scratch
+  unsigned long long *d_work = nullptr;  // [0] work counter, [1..7] stats, [8] clock scratch
+  int *d_error = nullptr;
+  double *d_rnd = nullptr;
+  size_t rnd_cap = 0;
+  int8_t *d_status = nullptr;
+  double *d_omc = nullptr;
+  uint32_t *d_steps = nullptr, *d_visits = nullptr;
+  size_t out_cap = 0;
+  // launch choice
+  int tuned_G = 0, tuned_block = 0;
+  ccs_stats last{};
+};
+
+namespace {
+
+int fail(ccs_ctx *c, int code, const char *fmt, ...) {
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return code;
+}
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(c, CCS_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),    \
+                  __FILE__, __LINE__);                                                 \
+  } while (0)
+
+template <typename P> void dfree(P *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+
+void free_target(ccs_ctx *c) {
+  dfree(c->d_xyzq32); dfree(c->d_ab32); dfree(c->d_abc32);
+  dfree(c->d_xyzq64); dfree(c->d_ab64); dfree(c->d_abc64);
+  dfree(c->d_cell_start);
+  c->have_target = false;
+  c->tuned_G = 0;
+}
+
+bool is_molecule(int gas) { return gas == CCS_GAS_N2 || gas == CCS_GAS_CO2; }
+int gas_kind(int gas) { return gas == CCS_GAS_N2 ? GAS_N2 : gas == CCS_GAS_CO2 ? GAS_CO2 : GAS_ATOM; }
+
+// GasBuffer::gas_properties (GasBuffer.cpp:58-192): site charges, masses, z offsets.
+void gas_table(int gas, double q[3], double m[3], double z[3], double &mass) {
+  for (int k = 0; k < 3; k++) q[k] = m[k] = z[k] = 0.0;
+  switch (gas) {
+    case CCS_GAS_HE: m[0] = 4.0026; mass = m[0]; break;
+    case CCS_GAS_AR: m[0] = 39.948; mass = m[0]; break;
+    case CCS_GAS_CO2_1SITE: m[0] = 44.0098; mass = m[0]; break;
+    case CCS_GAS_N2:
+      z[0] = 0.5488; z[1] = -0.5488; q[0] = q[1] = -0.4825; q[2] = 0.965;
+      m[0] = m[1] = 14.007; mass = m[0] + m[1];
+      break;
+    default:  // CO2
+      z[0] = -1.149; z[2] = 1.149; q[0] = q[2] = -0.3256; q[1] = 0.6512;
+      m[0] = m[2] = 15.999; m[1] = 12.011; mass = m[0] + m[1] + m[2];
+      break;
+  }
+}
+
+// Speed sampler table of System::velGenerator (System.cpp:1523-1555): the
+// same running sums in the same order, so a binary search for the first
+// S[k] >= u returns the speed the reference's linear scan returns.
+void vel_table(double m_amu, double T, std::vector<double> &V, std::vector<double> &S) {
+  const double AMU_TO_KG = 1.66053904E-27, KB = 1.38064E-23, ANG_TO_M = 1.0E-10, FS_TO_S = 1.0E-15;
+  auto distr = [&](double v) {
+    double m = m_amu * AMU_TO_KG;
+    v = v * ANG_TO_M / FS_TO_S;
+    return std::pow(v, 5.0) * std::pow((m / (2.0 * KB * T)), 3.0) *
+           std::exp(-(m * std::pow(v, 2.0)) / (2.0 * KB * T));
+  };
+  V.clear(); S.clear();
+  double v = 0.0, dv = 1.0E-5, s = distr(v);
+  V.push_back(v); S.push_back(s);
+  // until the CDF covers u = 1, or the density underflows (then the last entry
+  // answers every larger u; the reference would scan forever there)
+  while (s < 1.0 && V.size() < 4000000) {
+    v += dv;
+    const double pv = distr(v);
+    s += pv;
+    V.push_back(v); S.push_back(s);
+    if (pv == 0.0 && v * ANG_TO_M / FS_TO_S > 1.0e3) break;
+  }
+}
+
+using KernelFn = void (*)(KParams);
+using ForceFn = void (*)(KParams, int, size_t, const double *, double *, double *, uint32_t *);
+
+template <typename T, int G, int GAS, bool HASQ> KernelFn traj_ptr() { return traj_kernel<T, G, GAS, HASQ>; }
+template <typename T, int G, int GAS, bool HASQ> ForceFn force_ptr() {
+  return force_points_kernel<T, G, GAS, HASQ>;
+}
+
+constexpr int NG = 6;  // G = 1,2,4,8,16,32
+int g_index(int G) { int i = 0; while ((1 << i) < G) i++; return i; }
+
+template <typename T, int GAS, bool HASQ> KernelFn pick_traj_g(int gi) {
+  switch (gi) {
+    case 0: return traj_ptr<T, 1, GAS, HASQ>();
+    case 1: return traj_ptr<T, 2, GAS, HASQ>();
+    case 2: return traj_ptr<T, 4, GAS, HASQ>();
+    case 3: return traj_ptr<T, 8, GAS, HASQ>();
+    case 4: return traj_ptr<T, 16, GAS, HASQ>();
+    default: return traj_ptr<T, 32, GAS, HASQ>();
+  }
+}
+template <typename T, int GAS, bool HASQ> ForceFn pick_force_g(int gi) {
+  switch (gi) {
+    case 0: return force_ptr<T, 1, GAS, HASQ>();
+    case 3: return force_ptr<T, 8, GAS, HASQ>();
+    default: return force_ptr<T, 32, GAS, HASQ>();
+  }
+}
+template <typename T> KernelFn pick_traj_t(int gas, bool hasq, int gi) {
+  if (gas == GAS_ATOM) return hasq ? pick_traj_g<T, GAS_ATOM, true>(gi) : pick_traj_g<T, GAS_ATOM, false>(gi);
+  if (gas == GAS_N2) return hasq ? pick_traj_g<T, GAS_N2, true>(gi) : pick_traj_g<T, GAS_N2, false>(gi);
+  return hasq ? pick_traj_g<T, GAS_CO2, true>(gi) : pick_traj_g<T, GAS_CO2, false>(gi);
+}
+template <typename T> ForceFn pick_force_t(int gas, bool hasq, int gi) {
+  if (gas == GAS_ATOM) return hasq ? pick_force_g<T, GAS_ATOM, true>(gi) : pick_force_g<T, GAS_ATOM, false>(gi);
+  if (gas == GAS_N2) return hasq ? pick_force_g<T, GAS_N2, true>(gi) : pick_force_g<T, GAS_N2, false>(gi);
+  return hasq ? pick_force_g<T, GAS_CO2, true>(gi) : pick_force_g<T, GAS_CO2, false>(gi);
+}
+KernelFn pick_traj(const ccs_ctx *c, int G) {
+  const int gas = gas_kind(c->p.gas);
+  const bool hasq = c->coul_on || c->dip_on;
+  return c->p.precision == CCS_PREC_FP64 ? pick_traj_t<double>(gas, hasq, g_index(G))
+                                         : pick_traj_t<float>(gas, hasq, g_index(G));
+}
+ForceFn pick_force(const ccs_ctx *c, int G) {
+  const int gas = gas_kind(c->p.gas);
+  const bool hasq = c->coul_on || c->dip_on;
+  return c->p.precision == CCS_PREC_FP64 ? pick_force_t<double>(gas, hasq, g_index(G))
+                                         : pick_force_t<float>(gas, hasq, g_index(G));
+}
+
+KParams base_params(const ccs_ctx *c) {
+  const ccs_params &p = c->p;
+  KParams k;
+  std::memset(&k, 0, sizeof k);
+  k.xyzq32 = c->d_xyzq32; k.ab32 = c->d_ab32; k.abc32 = c->d_abc32 ? c->d_abc32 : c->d_ab32;
+  k.xyzq64 = c->d_xyzq64; k.ab64 = c->d_ab64; k.abc64 = c->d_abc64 ? c->d_abc64 : c->d_ab64;
+  k.cell_start = c->d_cell_start;
+  k.nx = c->nx; k.ny = c->ny; k.nz = c->nz; k.natoms = c->natoms;
+  k.ox = c->origin[0]; k.oy = c->origin[1]; k.oz = c->origin[2];
+  k.h = c->h; k.inv_h = 1.0 / c->h;
+  for (int d = 0; d < 3; d++) { k.bb_lo[d] = c->bb_lo[d]; k.bb_hi[d] = c->bb_hi[d]; }
+  k.reach = c->reach;
+  k.allpairs = c->allpairs;
+  k.coul_on = c->coul_on;
+  k.dip_on = c->dip_on;
+  double gq[3], gm[3], gz[3], gmass;
+  gas_table(p.gas, gq, gm, gz, gmass);
+  for (int s = 0; s < 3; s++) { k.q_site[s] = gq[s]; k.gas_m[s] = gm[s]; k.gas_z[s] = gz[s]; }
+  k.gas_mass = gmass;
+  if (c->allpairs) {
+    k.rlj2 = INFINITY; k.rc2 = INFINITY;
+    k.rc6inv = k.rc12inv = k.rc3inv = k.c1 = k.c2 = 0.0;
+  } else {
+    const double rl = p.lj_cutoff, rc = p.coul_cutoff;
+    k.rlj2 = rl * rl;
+    k.rc2 = rc * rc;
+    k.rc6inv = 1.0 / std::pow(rl, 6);
+    k.rc12inv = k.rc6inv * k.rc6inv;
+    k.rc3inv = 1.0 / std::pow(rc, 3);
+    k.c1 = 1.5 / rc;
+    k.c2 = 0.5 / std::pow(rc, 3);
+  }
+  k.alpha = p.alpha;
+  // reference grid: cells of lj_cutoff + skin over the box (LinkedCell.cpp:48-90)
+  const double rh = p.lj_cutoff + p.skin;
+  k.ref_h = rh;
+  k.ref_nx = (int)std::ceil(2.0 * p.a / rh);
+  k.ref_ny = (int)std::ceil(2.0 * p.b / rh);
+  k.ref_nz = (int)std::ceil(2.0 * p.c / rh);
+  k.ref_corner[0] = -0.5 * (k.ref_nx * rh);
+  k.ref_corner[1] = -0.5 * (k.ref_ny * rh);
+  k.ref_corner[2] = -0.5 * (k.ref_nz * rh);
+  k.ref_check = c->allpairs ? 0 : 1;
+  k.gas = p.gas;
+  k.dt = p.dt; k.mu = p.mu; k.temperature = p.temperature; k.gas_inertia = p.gas_inertia;
+  k.d_bond = p.d_bond; k.a = p.a; k.b = p.b; k.c = p.c; k.bmax = p.bmax;
+  k.lx = p.lx; k.ly = p.ly; k.lz = p.lz;
+  k.etol = p.gas == CCS_GAS_N2 ? 1.0 : p.gas == CCS_GAS_CO2 ? 20.0 : 0.5;
+  k.quirks = p.quirks;
+  k.max_steps = p.max_steps_per_try ? p.max_steps_per_try : 2000000u;
+  k.vtab_v = c->d_vtab_v; k.vtab_s = c->d_vtab_s; k.vtab_n = c->vtab_n;
+  k.work = c->d_work;
+  k.stats = c->d_work + 1;
+  k.error = c->d_error;
+  return k;
+}
+
+int ensure_run_buffers(ccs_ctx *c, size_t n, bool need_rnd) {
+  if (need_rnd && n > c->rnd_cap) {
+    dfree(c->d_rnd);
+    CK(cudaMalloc(&c->d_rnd, 9 * n * sizeof(double)));
+    CK(cudaMemsetAsync(c->d_rnd, 0, 9 * n * sizeof(double), c->stream));
+    c->rnd_cap = n;
+  }
+  if (n > c->out_cap) {
+    dfree(c->d_status); dfree(c->d_omc); dfree(c->d_steps); dfree(c->d_visits);
+    CK(cudaMalloc(&c->d_status, n));
+    CK(cudaMalloc(&c->d_omc, n * sizeof(double)));
+    CK(cudaMalloc(&c->d_steps, n * sizeof(uint32_t)));
+    CK(cudaMalloc(&c->d_visits, n * sizeof(uint32_t)));
+    c->out_cap = n;
+  }
+  return CCS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// device clock helper: one-thread kernel reading %globaltimer
+__global__ void read_globaltimer(unsigned long long *out) { *out = global_ns(); }
+
+namespace {
+int device_now_ns(ccs_ctx *c, unsigned long long &t) {
+  read_globaltimer<<<1, 1, 0, c->stream>>>(c->d_work + 8);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(&t, c->d_work + 8, sizeof t, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return CCS_OK;
+}
+
+// Full asynchronous run on device buffers (the kernel's only host sync is the
+// watchdog clock read at the start).
+int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t *d_status,
+               double *d_omc, uint32_t *d_steps, uint32_t *d_visits, cudaStream_t s, int G,
+               int block) {
+  KParams k = base_params(c);
+  k.rnd = d_rnd;
+  k.rnd_stride = stride;
+  k.ntraj = n;
+  k.status = d_status;
+  k.omc = d_omc;
+  k.steps = d_steps;
+  k.visits = d_visits;
+  unsigned long long now = 0;
+  int rc = device_now_ns(c, now);
+  if (rc) return rc;
+  const double wd = c->p.watchdog_s > 0 ? c->p.watchdog_s : 600.0;
+  KernelFn fn = pick_traj(c, G);
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, 0));
+  if (per_sm < 1) per_sm = 1;
+  size_t grid = (size_t)per_sm * c->sm_count;
+  const size_t max_useful = (n * (size_t)G + block - 1) / block;
+  if (grid > max_useful) grid = std::max<size_t>(1, max_useful);
+  k.deadline_ns = now + (unsigned long long)(wd * 1e9);
+  // d_work: [0] work counter, [1..7] statistics, [8] clock scratch
+  CK(cudaMemsetAsync(c->d_work, 0, 8 * sizeof(unsigned long long), s));
+  CK(cudaMemsetAsync(c->d_error, 0, sizeof(int), s));
+  fn<<<(unsigned)grid, block, 0, s>>>(k);
+  CK(cudaGetLastError());
+  c->last.grid_size = (int32_t)grid;
+  c->last.block_size = block;
+  c->last.lanes_per_traj = G;
+  return CCS_OK;
+}
+
+int read_stats(ccs_ctx *c, ccs_stats *st, size_t n) {
+  unsigned long long h[7];
+  int herr = 0;
+  CK(cudaMemcpyAsync(h, c->d_work + 1, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&herr, c->d_error, sizeof herr, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->last.ntraj = n;
+  c->last.nfree = h[0]; c->last.nscatter = h[1]; c->last.nlost = h[2]; c->last.ncapped = h[3];
+  c->last.steps = h[4]; c->last.visits = h[5]; c->last.force_calls = h[6];
+  if (st) *st = c->last;
+  if (herr) return fail(c, CCS_ERR_TIMEOUT, "device watchdog expired after %.0f s",
+                        c->p.watchdog_s > 0 ? c->p.watchdog_s : 600.0);
+  return CCS_OK;
+}
+
+// Autotuner: times each lanes-per-trajectory choice on a slice of the run and
+// keeps the fastest (trajectories are independent, so a slice is a fair sample).
+int autotune(ccs_ctx *c, size_t n, size_t stride, int block) {
+  if (c->p.lanes_per_traj > 0) { c->tuned_G = c->p.lanes_per_traj; c->tuned_block = block; return CCS_OK; }
+  if (c->tuned_G) return CCS_OK;
+  const int cand[4] = {1, 4, 8, 32};
+  size_t slice = std::min<size_t>(n, (size_t)c->sm_count * 64);
+  float best = 1e30f;
+  int bestG = 32;
+  for (int G : cand) {
+    for (int rep = 0; rep < 2; rep++) {  // first pass warms caches and code
+      CK(cudaEventRecord(c->ev[4], c->stream));
+      int rc = run_device(c, slice, c->d_rnd, stride, c->d_status, c->d_omc, nullptr, nullptr,
+                          c->stream, G, block);
+      if (rc) return rc;
+      CK(cudaEventRecord(c->ev[5], c->stream));
+      CK(cudaEventSynchronize(c->ev[5]));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
+      if (rep == 1 && ms < best) { best = ms; bestG = G; }
+    }
+  }
+  c->tuned_G = bestG;
+  c->tuned_block = block;
+  return CCS_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int ccs_version(int32_t *abi) {
+  if (abi) *abi = CCS_ABI_VERSION;
+  return CCS_OK;
+}
+
+void ccs_params_default(ccs_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof *p);
+  p->gas = CCS_GAS_HE;
+  p->force_type = 4;
+  p->dt = 10.0;           // Constants.h:72
+  p->temperature = 298.0; // Constants.h:73
+  p->lj_cutoff = 12.0;    // Constants.h:75
+  p->coul_cutoff = 25.0;  // Constants.h:77
+  p->skin = 0.01;         // Constants.h:74
+  p->precision = CCS_PREC_FP32;
+  p->watchdog_s = 600.0;
+}
+
+int ccs_create(ccs_ctx **out, int device) {
+  if (!out) return CCS_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return CCS_ERR_NODEVICE; }
+  if (device < 0 || device >= ndev) return CCS_ERR_INVALID;
+  ccs_ctx *c = new (std::nothrow) ccs_ctx();
+  if (!c) return CCS_ERR_NOMEM;
+  ccs_params_default(&c->p);
+  c->device = device;
+  auto bail = [&](int code) { ccs_destroy(c); return code; };
+  if (cudaSetDevice(device) != cudaSuccess) return bail(CCS_ERR_CUDA);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return bail(CCS_ERR_CUDA);
+  if (prop.major < 10) return bail(CCS_ERR_NODEVICE);  // built for sm_100a only
+  c->sm_count = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(CCS_ERR_CUDA);
+  for (auto &e : c->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return bail(CCS_ERR_CUDA);
+  if (cudaMalloc(&c->d_work, 9 * sizeof(unsigned long long)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
+  if (cudaMalloc(&c->d_error, sizeof(int)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
+  *out = c;
+  return CCS_OK;
+}
+
+void ccs_destroy(ccs_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_target(c);
+  dfree(c->d_vtab_v); dfree(c->d_vtab_s);
+  dfree(c->d_work); dfree(c->d_error); dfree(c->d_rnd);
+  dfree(c->d_status); dfree(c->d_omc); dfree(c->d_steps); dfree(c->d_visits);
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int ccs_set_params(ccs_ctx *c, const ccs_params *p) {
+  if (!c || !p) return CCS_ERR_INVALID;
+  if (p->gas < 1 || p->gas > 5) return fail(c, CCS_ERR_INVALID, "gas must be 1..5");
+  if (p->force_type < 1 || p->force_type > 6) return fail(c, CCS_ERR_INVALID, "force_type must be 1..6");
+  if (!is_molecule(p->gas) && p->force_type > 4)
+    return fail(c, CCS_ERR_INVALID, "atomic gases use force_type 1..4");
+  if (!(p->dt > 0) || !(p->temperature > 0) || !(p->mu > 0) || !(p->bmax > 0) || !(p->a > 0) ||
+      !(p->b > 0) || !(p->c > 0) || !(p->lx > 0) || !(p->ly > 0) || !(p->lz > 0))
+    return fail(c, CCS_ERR_INVALID, "dt, temperature, mu, a, b, c, bmax and box must be positive");
+  if (!(p->lj_cutoff > 0) || !(p->coul_cutoff > 0))
+    return fail(c, CCS_ERR_INVALID, "cutoffs must be positive");
+  if (is_molecule(p->gas) && (!(p->gas_inertia > 0) || !(p->d_bond > 0)))
+    return fail(c, CCS_ERR_INVALID, "molecular gases need gas_inertia and d_bond");
+  if (p->precision != CCS_PREC_FP32 && p->precision != CCS_PREC_FP64)
+    return fail(c, CCS_ERR_INVALID, "precision must be FP32 or FP64");
+  const int G = p->lanes_per_traj;
+  if (G != 0 && G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32)
+    return fail(c, CCS_ERR_INVALID, "lanes_per_traj must be 0 or a power of two up to 32");
+  if (p->block_size != 0 && (p->block_size % 32 || p->block_size > MAX_BLOCK || p->block_size < 32))
+    return fail(c, CCS_ERR_INVALID, "block_size must be a multiple of 32 up to %d", MAX_BLOCK);
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
+  const bool vel_changed = !c->have_params || c->p.mu != p->mu || c->p.temperature != p->temperature;
+  c->p = *p;
+  c->have_params = true;
+  free_target(c);
+  if (vel_changed) {
+    std::vector<double> V, S;
+    vel_table(p->mu, p->temperature, V, S);
+    dfree(c->d_vtab_v); dfree(c->d_vtab_s);
+    CK(cudaMalloc(&c->d_vtab_v, V.size() * sizeof(double)));
+    CK(cudaMalloc(&c->d_vtab_s, S.size() * sizeof(double)));
+    CK(cudaMemcpy(c->d_vtab_v, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_vtab_s, S.data(), S.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c->vtab_n = (int)V.size();
+  }
+  return CCS_OK;
+}
+
+int ccs_set_target(ccs_ctx *c, size_t n, const double *x, const double *y, const double *z,
+                   const double *q, const double *eps, const double *sig, const double *eps_c,
+                   const double *sig_c) {
+  if (!c) return CCS_ERR_INVALID;
+  if (!c->have_params) return fail(c, CCS_ERR_INVALID, "ccs_set_params must come first");
+  if (n == 0 || !x || !y || !z || !q || !eps || !sig)
+    return fail(c, CCS_ERR_INVALID, "target arrays missing or empty");
+  if (n > (size_t)1 << 30) return fail(c, CCS_ERR_INVALID, "too many atoms");
+  const ccs_params &p = c->p;
+  if (p.gas == CCS_GAS_CO2 && (!eps_c || !sig_c))
+    return fail(c, CCS_ERR_INVALID, "CO2 needs the carbon-site eps_c/sig_c");
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
+  free_target(c);
+  const int ft = p.force_type;
+  bool charged = false;
+  for (size_t i = 0; i < n; i++) {
+    if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(z[i]) || !std::isfinite(q[i]))
+      return fail(c, CCS_ERR_INVALID, "non-finite target coordinate or charge at atom %zu", i);
+    charged |= q[i] != 0.0;
+  }
+  const bool mol = is_molecule(p.gas);
+  c->charged = charged;
+  c->allpairs = (ft == 1 || ft == 3 || ft == 5);
+  c->coul_on = mol && ft >= 3 && charged;
+  c->dip_on = charged && (mol ? (ft == 5 || ft == 6) : (ft == 3 || ft == 4));
+  const bool hasq = c->coul_on || c->dip_on;
+  c->reach = std::max(p.lj_cutoff, hasq ? p.coul_cutoff : 0.0);
+  // engine cell edge: a fraction of the reach keeps the clipped columns close
+  // to the cutoff sphere; the autotuner picks lanes per trajectory on top
+  double h = p.cell_size > 0 ? p.cell_size : std::min(6.0, std::max(2.5, c->reach / 6.0));
+  double lo[3] = {x[0], y[0], z[0]}, hi[3] = {x[0], y[0], z[0]};
+  for (size_t i = 0; i < n; i++) {
+    lo[0] = std::min(lo[0], x[i]); hi[0] = std::max(hi[0], x[i]);
+    lo[1] = std::min(lo[1], y[i]); hi[1] = std::max(hi[1], y[i]);
+    lo[2] = std::min(lo[2], z[i]); hi[2] = std::max(hi[2], z[i]);
+  }
+  int dims[3];
+  for (int d = 0; d < 3; d++) {
+    c->bb_lo[d] = lo[d];
+    c->bb_hi[d] = hi[d];
+    c->origin[d] = lo[d] - 1e-6;
+    dims[d] = (int)std::floor((hi[d] - c->origin[d]) / h) + 1;
+  }
+  const long long ncell = (long long)dims[0] * dims[1] * dims[2];
+  if (ncell > (1ll << 28)) return fail(c, CCS_ERR_INVALID, "engine grid too large; raise cell_size");
+  c->nx = dims[0]; c->ny = dims[1]; c->nz = dims[2]; c->h = h; c->natoms = (int)n;
+  // counting sort by flat cell (i*ny + j)*nz + k, stable in input order
+  std::vector<int> cell(n), start((size_t)ncell + 1, 0), order(n);
+  for (size_t i = 0; i < n; i++) {
+    int ijk[3];
+    const double v[3] = {x[i], y[i], z[i]};
+    for (int d = 0; d < 3; d++)
+      ijk[d] = std::min(dims[d] - 1, std::max(0, (int)std::floor((v[d] - c->origin[d]) / h)));
+    cell[i] = (ijk[0] * c->ny + ijk[1]) * c->nz + ijk[2];
+    start[(size_t)cell[i] + 1]++;
+  }
+  for (long long k = 0; k < ncell; k++) start[(size_t)k + 1] += start[(size_t)k];
+  std::vector<int> fill(start.begin(), start.end() - 1);
+  for (size_t i = 0; i < n; i++) order[(size_t)fill[(size_t)cell[i]]++] = (int)i;
+  c->max_cell = 0;
+  for (long long k = 0; k < ncell; k++) c->max_cell = std::max(c->max_cell, start[(size_t)k + 1] - start[(size_t)k]);
+  // packed atom tables: A = 4 eps sig^12, B = 4 eps sig^6 (the lj2, lj1 of Force.cpp:89-90)
+  std::vector<float4> xq32(n);
+  std::vector<float2> ab32(n), abc32(p.gas == CCS_GAS_CO2 ? n : 0);
+  std::vector<double4> xq64(n);
+  std::vector<double2> ab64(n), abc64(p.gas == CCS_GAS_CO2 ? n : 0);
+  for (size_t s = 0; s < n; s++) {
+    const int i = order[s];
+    const double qq = (ft == 1 || ft == 2) ? 0.0 : q[i];
+    xq64[s] = make_double4(x[i], y[i], z[i], qq);
+    xq32[s] = make_float4((float)x[i], (float)y[i], (float)z[i], (float)qq);
+    const double s6 = std::pow(sig[i], 6.0), B = 4.0 * eps[i] * s6, A = B * s6;
+    ab64[s] = make_double2(A, B);
+    ab32[s] = make_float2((float)A, (float)B);
+    if (p.gas == CCS_GAS_CO2) {
+      const double c6 = std::pow(sig_c[i], 6.0), Bc = 4.0 * eps_c[i] * c6, Ac = Bc * c6;
+      abc64[s] = make_double2(Ac, Bc);
+      abc32[s] = make_float2((float)Ac, (float)Bc);
+    }
+  }
+  const bool fp64 = p.precision == CCS_PREC_FP64;
+  if (fp64) {
+    CK(cudaMalloc(&c->d_xyzq64, n * sizeof(double4)));
+    CK(cudaMalloc(&c->d_ab64, n * sizeof(double2)));
+    CK(cudaMemcpy(c->d_xyzq64, xq64.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_ab64, ab64.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+    if (p.gas == CCS_GAS_CO2) {
+      CK(cudaMalloc(&c->d_abc64, n * sizeof(double2)));
+      CK(cudaMemcpy(c->d_abc64, abc64.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+    }
+  } else {
+    CK(cudaMalloc(&c->d_xyzq32, n * sizeof(float4)));
+    CK(cudaMalloc(&c->d_ab32, n * sizeof(float2)));
+    CK(cudaMemcpy(c->d_xyzq32, xq32.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->d_ab32, ab32.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    if (p.gas == CCS_GAS_CO2) {
+      CK(cudaMalloc(&c->d_abc32, n * sizeof(float2)));
+      CK(cudaMemcpy(c->d_abc32, abc32.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    }
+  }
+  CK(cudaMalloc(&c->d_cell_start, start.size() * sizeof(int)));
+  CK(cudaMemcpy(c->d_cell_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+  c->have_target = true;
+  c->tuned_G = 0;
+  return CCS_OK;
+}
+
+int ccs_get_info(ccs_ctx *c, ccs_info *info) {
+  if (!c || !info) return CCS_ERR_INVALID;
+  std::memset(info, 0, sizeof *info);
+  info->nx = c->nx; info->ny = c->ny; info->nz = c->nz; info->natoms = c->natoms;
+  info->cell_size = c->h; info->reach = c->reach;
+  for (int d = 0; d < 3; d++) info->origin[d] = c->origin[d];
+  info->charged = c->charged; info->allpairs = c->allpairs; info->max_cell_atoms = c->max_cell;
+  info->vel_table_len = c->vtab_n; info->sm_count = c->sm_count;
+  info->reserved = c->tuned_G;
+  return CCS_OK;
+}
+
+int ccs_run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t *d_status,
+                   double *d_omc, uint32_t *d_steps, uint32_t *d_visits, void *stream) {
+  if (!c) return CCS_ERR_INVALID;
+  if (!c->have_target) return fail(c, CCS_ERR_INVALID, "no target set");
+  if (n == 0) return CCS_OK;
+  if (!d_rnd || !d_status || !d_omc || stride < n) return fail(c, CCS_ERR_INVALID, "bad device buffers");
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  const int block = c->p.block_size ? c->p.block_size : 128;
+  if (!c->tuned_G) {
+    // tune on the caller's inputs (outputs land in the context's own buffers)
+    int rc = ensure_run_buffers(c, std::min<size_t>(n, (size_t)c->sm_count * 64), false);
+    if (rc) return rc;
+    if (c->p.lanes_per_traj > 0) c->tuned_G = c->p.lanes_per_traj;
+    else {
+      CK(cudaStreamSynchronize(s));
+      const double *save = c->d_rnd;
+      c->d_rnd = const_cast<double *>(d_rnd);
+      rc = autotune(c, n, stride, block);
+      c->d_rnd = const_cast<double *>(save);
+      if (rc) return rc;
+    }
+  }
+  CK(cudaEventRecord(c->ev[2], s));
+  int rc = run_device(c, n, d_rnd, stride, d_status, d_omc, d_steps, d_visits, s, c->tuned_G, block);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev[3], s));
+  c->last.ntraj = n;
+  return CCS_OK;
+}
+
+int ccs_sync_stats(ccs_ctx *c, ccs_stats *st) {
+  if (!c) return CCS_ERR_INVALID;
+  CK(cudaEventSynchronize(c->ev[3]));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
+  c->last.kernel_ms = ms;
+  return read_stats(c, st, c->last.ntraj);
+}
+
+int ccs_run(ccs_ctx *c, size_t n, const double *const rnd[9], int8_t *status, double *omc,
+            uint32_t *steps, uint32_t *visits, ccs_stats *st) {
+  if (!c) return CCS_ERR_INVALID;
+  if (!c->have_target) return fail(c, CCS_ERR_INVALID, "no target set");
+  if (n == 0) { if (st) { std::memset(st, 0, sizeof *st); } return CCS_OK; }
+  if (!rnd || !status || !omc) return fail(c, CCS_ERR_INVALID, "rnd, status and one_minus_cos are required");
+  const int nrows = is_molecule(c->p.gas) ? 9 : 5;
+  for (int k = 0; k < nrows; k++)
+    if (!rnd[k]) return fail(c, CCS_ERR_INVALID, "rnd[%d] is NULL", k);
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
+  int rc = ensure_run_buffers(c, n, true);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  for (int k = 0; k < nrows; k++)
+    CK(cudaMemcpyAsync(c->d_rnd + (size_t)k * n, rnd[k], n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  const int block = c->p.block_size ? c->p.block_size : 128;
+  rc = autotune(c, n, n, block);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev[2], c->stream));
+  rc = run_device(c, n, c->d_rnd, n, c->d_status, c->d_omc, steps ? c->d_steps : nullptr,
+                  visits ? c->d_visits : nullptr, c->stream, c->tuned_G, block);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev[3], c->stream));
+  CK(cudaMemcpyAsync(status, c->d_status, n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(omc, c->d_omc, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (steps) CK(cudaMemcpyAsync(steps, c->d_steps, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  if (visits) CK(cudaMemcpyAsync(visits, c->d_visits, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaEventRecord(c->ev[4], c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  float t01 = 0, t23 = 0, t34 = 0;
+  CK(cudaEventElapsedTime(&t01, c->ev[0], c->ev[1]));
+  CK(cudaEventElapsedTime(&t23, c->ev[2], c->ev[3]));
+  CK(cudaEventElapsedTime(&t34, c->ev[3], c->ev[4]));
+  c->last.h2d_ms = t01;
+  c->last.kernel_ms = t23;
+  c->last.d2h_ms = t34;
+  return read_stats(c, st, n);
+}
+
+int ccs_eval_site_forces(ccs_ctx *c, size_t npts, int site, const double *pos, double *f, double *U,
+                         uint32_t *visits) {
+  if (!c) return CCS_ERR_INVALID;
+  if (!c->have_target) return fail(c, CCS_ERR_INVALID, "no target set");
+  const int ns = is_molecule(c->p.gas) ? 3 : 1;
+  if (site < 0 || site >= ns) return fail(c, CCS_ERR_INVALID, "site out of range");
+  if (npts == 0) return CCS_OK;
+  if (!pos || !f || !U) return fail(c, CCS_ERR_INVALID, "pos, f and U are required");
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
+  double *dp = nullptr, *df = nullptr, *dU = nullptr;
+  uint32_t *dv = nullptr;
+  auto cleanup = [&]() { cudaFree(dp); cudaFree(df); cudaFree(dU); cudaFree(dv); };
+  if (cudaMalloc(&dp, npts * 3 * sizeof(double)) || cudaMalloc(&df, npts * 3 * sizeof(double)) ||
+      cudaMalloc(&dU, npts * sizeof(double)) || cudaMalloc(&dv, npts * sizeof(uint32_t))) {
+    cleanup();
+    return fail(c, CCS_ERR_NOMEM, "cudaMalloc for force points");
+  }
+  int rc = CCS_OK;
+  do {
+    if (cudaMemcpy(dp, pos, npts * 3 * sizeof(double), cudaMemcpyHostToDevice)) { rc = CCS_ERR_CUDA; break; }
+    KParams k = base_params(c);
+    const int G = c->p.lanes_per_traj == 1 ? 1 : c->p.lanes_per_traj == 8 ? 8 : 32;
+    ForceFn fn = pick_force(c, G);
+    const int block = 128;
+    const size_t grid = std::min<size_t>((npts * G + block - 1) / block, (size_t)c->sm_count * 16);
+    fn<<<(unsigned)grid, block, 0, c->stream>>>(k, site, npts, dp, df, dU, dv);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) { rc = CCS_ERR_CUDA; break; }
+    if (cudaMemcpy(f, df, npts * 3 * sizeof(double), cudaMemcpyDeviceToHost) ||
+        cudaMemcpy(U, dU, npts * sizeof(double), cudaMemcpyDeviceToHost)) { rc = CCS_ERR_CUDA; break; }
+    if (visits && cudaMemcpy(visits, dv, npts * sizeof(uint32_t), cudaMemcpyDeviceToHost)) { rc = CCS_ERR_CUDA; break; }
+  } while (0);
+  cleanup();
+  if (rc) return fail(c, rc, "force evaluation failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return CCS_OK;
+}
+
+int ccs_eval_setup(ccs_ctx *c, size_t n, const double *const rnd[9], int8_t *hit, double *pos, double *vel) {
+  if (!c) return CCS_ERR_INVALID;
+  if (!c->have_params || !c->vtab_n) return fail(c, CCS_ERR_INVALID, "ccs_set_params must come first");
+  if (n == 0) return CCS_OK;
+  if (!rnd || !hit || !pos || !vel) return fail(c, CCS_ERR_INVALID, "missing buffers");
+  const int nrows = is_molecule(c->p.gas) ? 9 : 5;
+  for (int k = 0; k < nrows; k++)
+    if (!rnd[k]) return fail(c, CCS_ERR_INVALID, "rnd[%d] is NULL", k);
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
+  int rc = ensure_run_buffers(c, n, true);
+  if (rc) return rc;
+  double *dpos = nullptr, *dvel = nullptr;
+  if (cudaMalloc(&dpos, n * 9 * sizeof(double)) || cudaMalloc(&dvel, n * 9 * sizeof(double))) {
+    cudaFree(dpos); cudaFree(dvel);
+    return fail(c, CCS_ERR_NOMEM, "cudaMalloc for setup");
+  }
+  for (int k = 0; k < nrows; k++)
+    if (cudaMemcpy(c->d_rnd + (size_t)k * n, rnd[k], n * sizeof(double), cudaMemcpyHostToDevice)) rc = CCS_ERR_CUDA;
+  if (!rc) {
+    KParams k = base_params(c);
+    k.rnd = c->d_rnd;
+    k.rnd_stride = n;
+    k.ntraj = n;
+    setup_kernel<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(k, c->d_status, dpos, dvel);
+    if (cudaGetLastError() || cudaStreamSynchronize(c->stream)) rc = CCS_ERR_CUDA;
+  }
+  if (!rc && (cudaMemcpy(hit, c->d_status, n, cudaMemcpyDeviceToHost) ||
+              cudaMemcpy(pos, dpos, n * 9 * sizeof(double), cudaMemcpyDeviceToHost) ||
+              cudaMemcpy(vel, dvel, n * 9 * sizeof(double), cudaMemcpyDeviceToHost)))
+    rc = CCS_ERR_CUDA;
+  cudaFree(dpos);
+  cudaFree(dvel);
+  if (rc) return fail(c, rc, "setup evaluation failed");
+  return CCS_OK;
+}
+
+const char *ccs_status_string(int s) {
+  switch (s) {
+    case CCS_OK: return "ok";
+    case CCS_ERR_INVALID: return "invalid argument";
+    case CCS_ERR_NOMEM: return "out of memory";
+    case CCS_ERR_CUDA: return "CUDA error";
+    case CCS_ERR_TIMEOUT: return "device watchdog expired";
+    case CCS_ERR_NODEVICE: return "no usable CUDA device";
+    case CCS_ERR_UNSUPPORTED: return "unsupported configuration";
+    default: return "unknown status";
+  }
+}
+
+const char *ccs_last_error(ccs_ctx *c) { return c ? c->err.c_str() : "no context"; }
+
+}  // extern "C"

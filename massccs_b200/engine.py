@@ -1,0 +1,252 @@
+"""ctypes binding of libmassccs_gpu.so (include/massccs_gpu.h).
+
+The Python face of the drop-in boundary: the same entry points a C/C++ host
+binds, with numpy arrays for the host buffers.  Loading fails loudly when the
+CUDA library is missing -- there is no CPU fallback in the product path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libmassccs_gpu.so")
+
+GAS = {"He": 1, "N2": 2, "CO2": 3, "Ar": 4, "co2": 5}
+PREC_FP32, PREC_FP64 = 0, 1
+QUIRK_CO2_VCM = 1
+STATUS_FREE, STATUS_SCATTER, STATUS_LOST, STATUS_CAPPED = 0, 1, 2, 3
+
+
+class CcsParams(ctypes.Structure):
+    _fields_ = [
+        ("gas", ctypes.c_int32), ("force_type", ctypes.c_int32),
+        ("dt", ctypes.c_double), ("temperature", ctypes.c_double), ("mu", ctypes.c_double),
+        ("gas_inertia", ctypes.c_double), ("d_bond", ctypes.c_double), ("alpha", ctypes.c_double),
+        ("lj_cutoff", ctypes.c_double), ("coul_cutoff", ctypes.c_double), ("skin", ctypes.c_double),
+        ("a", ctypes.c_double), ("b", ctypes.c_double), ("c", ctypes.c_double),
+        ("bmax", ctypes.c_double),
+        ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+        ("precision", ctypes.c_int32), ("quirks", ctypes.c_int32),
+        ("cell_size", ctypes.c_double),
+        ("lanes_per_traj", ctypes.c_int32), ("block_size", ctypes.c_int32),
+        ("max_steps_per_try", ctypes.c_uint32),
+        ("watchdog_s", ctypes.c_double),
+    ]
+
+
+class CcsStats(ctypes.Structure):
+    _fields_ = [
+        ("ntraj", ctypes.c_uint64), ("nfree", ctypes.c_uint64), ("nscatter", ctypes.c_uint64),
+        ("nlost", ctypes.c_uint64), ("ncapped", ctypes.c_uint64),
+        ("steps", ctypes.c_uint64), ("visits", ctypes.c_uint64), ("force_calls", ctypes.c_uint64),
+        ("kernel_ms", ctypes.c_double), ("h2d_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double),
+        ("lanes_per_traj", ctypes.c_int32), ("block_size", ctypes.c_int32),
+        ("grid_size", ctypes.c_int32), ("reserved", ctypes.c_int32),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class CcsInfo(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("natoms", ctypes.c_int32),
+        ("cell_size", ctypes.c_double), ("reach", ctypes.c_double),
+        ("origin", ctypes.c_double * 3),
+        ("charged", ctypes.c_int32), ("allpairs", ctypes.c_int32),
+        ("max_cell_atoms", ctypes.c_int32), ("vel_table_len", ctypes.c_int32),
+        ("sm_count", ctypes.c_int32), ("reserved", ctypes.c_int32),
+    ]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["origin"] = list(self.origin)
+        d["lanes_per_traj"] = self.reserved
+        return d
+
+
+# Every symbol include/massccs_gpu.h declares.
+EXPORTS = ["ccs_version", "ccs_create", "ccs_destroy", "ccs_params_default", "ccs_set_target",
+           "ccs_set_params", "ccs_run", "ccs_run_device", "ccs_sync_stats", "ccs_eval_site_forces",
+           "ccs_eval_setup", "ccs_get_info", "ccs_status_string", "ccs_last_error"]
+
+_LIB = None
+
+
+def load_library(path=LIB_PATH):
+    """Load the engine library (no GPU needed to load it)."""
+    global _LIB
+    if _LIB is not None and path == LIB_PATH:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"massccs_b200: CUDA engine library missing at {path}; "
+                           "build it with `python -m massccs_b200.build`")
+    L = ctypes.CDLL(path)
+    vp, sz, i32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int
+    L.ccs_version.argtypes = [ctypes.POINTER(ctypes.c_int32)]
+    L.ccs_create.argtypes = [ctypes.POINTER(vp), i32]
+    L.ccs_destroy.argtypes = [vp]
+    L.ccs_destroy.restype = None
+    L.ccs_params_default.argtypes = [ctypes.POINTER(CcsParams)]
+    L.ccs_params_default.restype = None
+    L.ccs_set_target.argtypes = [vp, sz] + [vp] * 8
+    L.ccs_set_params.argtypes = [vp, ctypes.POINTER(CcsParams)]
+    L.ccs_run.argtypes = [vp, sz, ctypes.POINTER(vp), vp, vp, vp, vp, ctypes.POINTER(CcsStats)]
+    L.ccs_run_device.argtypes = [vp, sz, vp, sz, vp, vp, vp, vp, vp]
+    L.ccs_sync_stats.argtypes = [vp, ctypes.POINTER(CcsStats)]
+    L.ccs_eval_site_forces.argtypes = [vp, sz, i32, vp, vp, vp, vp]
+    L.ccs_eval_setup.argtypes = [vp, sz, ctypes.POINTER(vp), vp, vp, vp]
+    L.ccs_get_info.argtypes = [vp, ctypes.POINTER(CcsInfo)]
+    L.ccs_status_string.argtypes = [i32]
+    L.ccs_status_string.restype = ctypes.c_char_p
+    L.ccs_last_error.argtypes = [vp]
+    L.ccs_last_error.restype = ctypes.c_char_p
+    if path == LIB_PATH:
+        _LIB = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def default_params(**kw):
+    p = CcsParams()
+    load_library().ccs_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+class CcsError(RuntimeError):
+    pass
+
+
+class Engine:
+    """One device context of the trajectory engine."""
+
+    def __init__(self, device=0):
+        self._L = load_library()
+        h = ctypes.c_void_p()
+        rc = self._L.ccs_create(ctypes.byref(h), device)
+        if rc != 0:
+            raise CcsError(f"ccs_create: {self._L.ccs_status_string(rc).decode()}")
+        self._h = h
+        self.gas = None
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = self._L.ccs_last_error(self._h).decode()
+            raise CcsError(f"{what}: {self._L.ccs_status_string(rc).decode()}: {msg}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.ccs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params=None, **kw):
+        p = params if params is not None else default_params()
+        for k, v in kw.items():
+            setattr(p, k, v)
+        self._check(self._L.ccs_set_params(self._h, ctypes.byref(p)), "ccs_set_params")
+        self.gas = p.gas
+        self.params = p
+        return p
+
+    def set_target(self, x, y, z, q, eps, sig, eps_c=None, sig_c=None):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else None
+                for a in (x, y, z, q, eps, sig, eps_c, sig_c)]
+        self._keep = arrs
+        n = arrs[0].shape[0]
+        self._check(self._L.ccs_set_target(self._h, n, *[_p(a) for a in arrs]), "ccs_set_target")
+
+    def info(self):
+        i = CcsInfo()
+        self._check(self._L.ccs_get_info(self._h, ctypes.byref(i)), "ccs_get_info")
+        return i.as_dict()
+
+    @staticmethod
+    def _rows(rnd):
+        rnd = np.ascontiguousarray(rnd, dtype=np.float64)
+        assert rnd.ndim == 2 and rnd.shape[0] == 9
+        ptrs = (ctypes.c_void_p * 9)(*[rnd[k].ctypes.data for k in range(9)])
+        return rnd, ptrs
+
+    def run(self, rnd, want_steps=True, want_visits=True):
+        """rnd: (9, n) array of the reference's pre-drawn values."""
+        rnd, ptrs = self._rows(rnd)
+        n = rnd.shape[1]
+        status = np.empty(n, dtype=np.int8)
+        omc = np.empty(n, dtype=np.float64)
+        steps = np.empty(n, dtype=np.uint32) if want_steps else None
+        visits = np.empty(n, dtype=np.uint32) if want_visits else None
+        st = CcsStats()
+        self._check(self._L.ccs_run(self._h, n, ptrs, _p(status), _p(omc), _p(steps), _p(visits),
+                                    ctypes.byref(st)), "ccs_run")
+        return {"status": status, "one_minus_cos": omc, "steps": steps, "visits": visits,
+                "stats": st.as_dict()}
+
+    def run_device(self, n, d_rnd, stride, d_status, d_omc, d_steps=0, d_visits=0, stream=0):
+        """Asynchronous run on device pointers (ints), e.g. torch tensors' data_ptr()."""
+        self._check(self._L.ccs_run_device(self._h, n, d_rnd, stride, d_status, d_omc,
+                                           d_steps or None, d_visits or None, stream or None),
+                    "ccs_run_device")
+
+    def sync_stats(self):
+        st = CcsStats()
+        self._check(self._L.ccs_sync_stats(self._h, ctypes.byref(st)), "ccs_sync_stats")
+        return st.as_dict()
+
+    def eval_site_forces(self, site, pos, want_visits=True):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        n = pos.shape[0]
+        f = np.empty((n, 3))
+        U = np.empty(n)
+        vis = np.empty(n, dtype=np.uint32) if want_visits else None
+        self._check(self._L.ccs_eval_site_forces(self._h, n, site, _p(pos), _p(f), _p(U), _p(vis)),
+                    "ccs_eval_site_forces")
+        return f, U, vis
+
+    def eval_setup(self, rnd):
+        rnd, ptrs = self._rows(rnd)
+        n = rnd.shape[1]
+        hit = np.empty(n, dtype=np.int8)
+        pos = np.empty((n, 3, 3))
+        vel = np.empty((n, 3, 3))
+        self._check(self._L.ccs_eval_setup(self._h, n, ptrs, _p(hit), _p(pos), _p(vel)),
+                    "ccs_eval_setup")
+        return hit, pos, vel
+
+
+def params_from_system(sp, precision=PREC_FP32, quirks=0, **kw):
+    """ccs_params from a dict of the reference's System scalars (keys as the
+    orc_params / massccs_host set-up report them)."""
+    p = default_params()
+    p.gas = int(sp["gas_flag"])
+    p.force_type = int(sp["force_type"])
+    p.dt = sp["dt"]
+    p.temperature = sp["temperature"]
+    p.mu = sp["mu"]
+    p.gas_inertia = sp.get("gas_inertia", 0.0)
+    p.d_bond = sp.get("d_bond", 0.0)
+    p.alpha = sp["alpha"]
+    p.lj_cutoff = sp["lj_cutoff"]
+    p.coul_cutoff = sp["coul_cutoff"]
+    p.skin = sp["skin"]
+    p.a, p.b, p.c, p.bmax = sp["a"], sp["b"], sp["c"], sp["bmax"]
+    p.lx, p.ly, p.lz = sp["lx"], sp["ly"], sp["lz"]
+    p.precision = precision
+    p.quirks = quirks
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
