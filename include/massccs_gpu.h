@@ -91,6 +91,8 @@ typedef struct {
   int32_t block_size;       /* 0 = automatic (multiple of 32) */
   uint32_t max_steps_per_try; /* 0 = 2,000,000 */
   double watchdog_s;        /* kernel wall-time budget, 0 = 600 s */
+  int32_t schedule;         /* 0 = index order, 1 = longest expected trajectories first */
+  uint32_t park_steps;      /* steps after which a trajectory moves to the warp pass; 0 = 2048 */
 } ccs_params;
 
 /* Per-run statistics. */
@@ -98,10 +100,11 @@ typedef struct {
   uint64_t ntraj, nfree, nscatter, nlost, ncapped;
   uint64_t steps;           /* integration steps, all tries */
   uint64_t visits;          /* site x atom pairs the engine evaluated */
-  uint64_t force_calls;     /* site force evaluations */
-  double kernel_ms;         /* device time of the trajectory kernel (CUDA events) */
+  uint64_t parked;          /* trajectories finished by the warp pass (the long ones) */
+  double kernel_ms;         /* device time of both trajectory passes (CUDA events) */
   double h2d_ms, d2h_ms;    /* copy times of ccs_run (CUDA events) */
   int32_t lanes_per_traj, block_size, grid_size, reserved;
+  double lane_ms, warp_ms;  /* the lane pass and the warp pass separately */
 } ccs_stats;
 
 typedef struct ccs_ctx ccs_ctx;

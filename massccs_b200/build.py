@@ -70,6 +70,8 @@ def build_host(force=False):
     if not os.path.isdir(hdir):
         return None
     cpp = sorted(os.path.join(hdir, f) for f in os.listdir(hdir) if f.endswith(".cpp") and f != "main.cpp")
+    if not cpp:
+        return None
     hdr = [os.path.join(hdir, f) for f in os.listdir(hdir) if f.endswith(".h")]
     lib_out = os.path.join(LIB, "libmassccs_host.so")
     deps = cpp + hdr + [os.path.join(INC, f) for f in os.listdir(INC)]

@@ -54,13 +54,16 @@ struct KParams {
   double q_site[3];
   double rlj2, rc2, rc6inv, rc12inv, rc3inv, c1, c2, alpha;
   // reference grid (LinkedCell.cpp:48-90) for the out-of-grid rule
-  double ref_corner[3], ref_h;
+  double ref_corner[3], ref_h, ref_inv_h;
   int ref_nx, ref_ny, ref_nz, ref_check;
   // dynamics
   int gas;                // ccs_gas numbering (1..5)
   double dt, mu, temperature, gas_inertia, d_bond, a, b, c, bmax, lx, ly, lz;
+  double inv_a, inv_b, inv_c;
   double gas_m[3], gas_z[3], gas_mass;
   double etol;            // energy tolerance in percent
+  // integrator constants of the moving pair (atoms: m1 = mu)
+  double half_kconv_over_m1, half_kconv_over_m2, inv_m1, inv_m2, mu12, mu12_over_m1, mu12_over_m2;
   int quirks;
   uint32_t max_steps;
   unsigned long long deadline_ns;
@@ -74,8 +77,15 @@ struct KParams {
   double *omc;
   uint32_t *steps;
   uint32_t *visits;
+  const uint32_t *order;      // processing order of the trajectories (longest expected first)
   unsigned long long *work;   // [0] next trajectory
-  unsigned long long *stats;  // nfree, nscatter, nlost, ncapped, steps, visits, force_calls
+  unsigned long long *stats;  // nfree, nscatter, nlost, ncapped, steps, visits, parked
+  // parking of long trajectories (lane pass -> warp pass)
+  void *park;                       // LaneState<T>[park_cap]
+  unsigned long long *park_count;   // parked so far
+  unsigned long long *park_next;    // next parked trajectory to resume
+  unsigned long long park_cap;
+  uint32_t park_steps;
   int *error;                 // 1 = watchdog
 };
 
@@ -85,19 +95,17 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Watchdog test with one answer for the whole group (lane 0 reads the clock),
-// so every lane of a group takes the same branch.
-template <int G>
-__device__ __forceinline__ bool group_expired(const KParams &kp, int g, unsigned mask);
-
 template <typename T> struct Real;
 template <> struct Real<float> {
   static __device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
   static __device__ __forceinline__ float sq(float x) { return sqrtf(x); }
+  // quotient for the FP32 integrator (2 ulp; the operands are O(1) and positive-definite)
+  static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
 };
 template <> struct Real<double> {
   static __device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
   static __device__ __forceinline__ double sq(double x) { return sqrt(x); }
+  static __device__ __forceinline__ double div(double a, double b) { return a / b; }
 };
 
 template <typename T> struct Atom { T x, y, z, q, A, B, Ac, Bc; };
@@ -211,12 +219,12 @@ __device__ __forceinline__ void visit_atom(const KParams &kp, const T (&p)[GasSh
 template <typename T>
 __device__ __forceinline__ bool ref_inside(const KParams &kp, T x, T y, T z) {
   if (!kp.ref_check) return true;
-  const double h = kp.ref_h;
-  const long i = (long)floor(((double)x - kp.ref_corner[0]) / h);
-  const long j = (long)floor(((double)y - kp.ref_corner[1]) / h);
-  const long k = (long)floor(((double)z - kp.ref_corner[2]) / h);
-  const long idx = k + (long)kp.ref_nz * j + (long)kp.ref_nz * kp.ref_ny * i;
-  return idx >= 0 && idx < (long)kp.ref_nx * kp.ref_ny * kp.ref_nz;
+  const T ih = T(kp.ref_inv_h);
+  const int i = (int)floor((x - T(kp.ref_corner[0])) * ih);
+  const int j = (int)floor((y - T(kp.ref_corner[1])) * ih);
+  const int k = (int)floor((z - T(kp.ref_corner[2])) * ih);
+  const long long idx = k + (long long)kp.ref_nz * j + (long long)kp.ref_nz * kp.ref_ny * i;
+  return idx >= 0 && idx < (long long)kp.ref_nx * kp.ref_ny * kp.ref_nz;
 }
 
 // Site forces of one probe configuration.  All G lanes of the group call it
@@ -251,11 +259,13 @@ __device__ __forceinline__ void eval_forces(const KParams &kp, const T (&p)[GasS
       const int j1 = (int)fmin(T(kp.ny - 1), floor((cy + R - oy) * ih));
       const int nj = j1 - j0 + 1;
       const int ncol = (i1 >= i0 && nj > 0) ? (i1 - i0 + 1) * nj : 0;
+      const float inv_nj = 1.0f / (float)(nj > 0 ? nj : 1);
       for (int base = 0; base < ncol; base += G) {
         const int cidx = base + g;
         int b = 0, len = 0;
         if (cidx < ncol) {
-          const int i = i0 + cidx / nj, j = j0 + cidx % nj;
+          const int di = (int)(((float)cidx + 0.5f) * inv_nj);  // exact: cidx < 2^20
+          const int i = i0 + di, j = j0 + (cidx - di * nj);
           const T xlo = ox + T(i) * h, ylo = oy + T(j) * h;
           const T dxc = fmax(fmax(xlo - cx, cx - (xlo + h)), T(0));
           const T dyc = fmax(fmax(ylo - cy, cy - (ylo + h)), T(0));
@@ -336,6 +346,158 @@ __device__ __forceinline__ void eval_forces(const KParams &kp, const T (&p)[GasS
   visits += nvis;
 }
 
+// Block-cooperative site forces for the warp pass: all NT threads of a CTA
+// evaluate one probe configuration.  Columns are split over the threads, the
+// run lengths are scanned block-wide, every thread visits candidates t, t+NT,
+// ... (two per iteration for instruction-level parallelism), and the sums are
+// reduced per warp (xor shuffles) and then across warps in shared memory in
+// a fixed order, so every thread ends with identical bits.
+template <typename T, int NT, int GAS, bool HASQ>
+__device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
+                                                  const bool (&act)[GasShape<GAS>::NS], const T (&cen)[3],
+                                                  T off, T (&f)[GasShape<GAS>::NS][3],
+                                                  T (&U)[GasShape<GAS>::NS], uint32_t &visits, int tid,
+                                                  int *sm_end, int *sm_del, int *sm_wsum, T *sm_red) {
+  constexpr int NS = GasShape<GAS>::NS;
+  constexpr int NW = NT / 32;
+  constexpr int NV = 4 * NS + 9;
+  const int lane = tid & 31, w = tid >> 5;
+  Acc<T, NS> acc;
+  acc.zero();
+  bool any = false;
+#pragma unroll
+  for (int s = 0; s < NS; s++) any |= act[s];
+  uint32_t nvis = 0;
+  if (any) {
+    const T R = kp.allpairs ? T(INFINITY) : T(kp.reach) + off + T(1e-3);
+    const T cx = cen[0], cy = cen[1], cz = cen[2];
+    const T ex = fmax(fmax(T(kp.bb_lo[0]) - cx, cx - T(kp.bb_hi[0])), T(0));
+    const T ey = fmax(fmax(T(kp.bb_lo[1]) - cy, cy - T(kp.bb_hi[1])), T(0));
+    const T ez = fmax(fmax(T(kp.bb_lo[2]) - cz, cz - T(kp.bb_hi[2])), T(0));
+    if (ex * ex + ey * ey + ez * ez <= R * R) {
+      const T ih = T(kp.inv_h), h = T(kp.h), ox = T(kp.ox), oy = T(kp.oy), oz = T(kp.oz);
+      const int i0 = (int)fmax(T(0), floor((cx - R - ox) * ih));
+      const int i1 = (int)fmin(T(kp.nx - 1), floor((cx + R - ox) * ih));
+      const int j0 = (int)fmax(T(0), floor((cy - R - oy) * ih));
+      const int j1 = (int)fmin(T(kp.ny - 1), floor((cy + R - oy) * ih));
+      const int nj = j1 - j0 + 1;
+      const int ncol = (i1 >= i0 && nj > 0) ? (i1 - i0 + 1) * nj : 0;
+      const float inv_nj = 1.0f / (float)(nj > 0 ? nj : 1);
+      for (int base = 0; base < ncol; base += NT) {
+        const int cidx = base + tid;
+        int b = 0, len = 0;
+        if (cidx < ncol) {
+          const int di = (int)(((float)cidx + 0.5f) * inv_nj);
+          const int i = i0 + di, j = j0 + (cidx - di * nj);
+          const T xlo = ox + T(i) * h, ylo = oy + T(j) * h;
+          const T dxc = fmax(fmax(xlo - cx, cx - (xlo + h)), T(0));
+          const T dyc = fmax(fmax(ylo - cy, cy - (ylo + h)), T(0));
+          const T rem = R * R - dxc * dxc - dyc * dyc;
+          if (rem >= T(0)) {
+            const T zr = Real<T>::sq(rem);
+            const int k0 = (int)fmax(T(0), floor((cz - zr - oz) * ih));
+            const int k1 = (int)fmin(T(kp.nz - 1), floor((cz + zr - oz) * ih));
+            if (k0 <= k1) {
+              const int cb = (i * kp.ny + j) * kp.nz;
+              b = __ldg(&kp.cell_start[cb + k0]);
+              len = __ldg(&kp.cell_start[cb + k1 + 1]) - b;
+            }
+          }
+        }
+        // block-wide inclusive scan of the run lengths
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        if (lane == 31) sm_wsum[w] = incl;
+        __syncthreads();
+        int wofs = 0, total = 0;
+#pragma unroll
+        for (int k = 0; k < NW; k++) {
+          const int ws = sm_wsum[k];
+          wofs += k < w ? ws : 0;
+          total += ws;
+        }
+        incl += wofs;
+        sm_end[tid] = incl;
+        sm_del[tid] = b - (incl - len);
+        __syncthreads();
+        if (total > 0) {
+          int r = 0, cur_end = sm_end[0], cur_del = sm_del[0];
+          int r2 = 0, cur_end2 = cur_end, cur_del2 = cur_del;
+          int t = tid;
+          for (; t + NT < total; t += 2 * NT) {
+            while (t >= cur_end) { ++r; cur_end = sm_end[r]; cur_del = sm_del[r]; }
+            const int t2 = t + NT;
+            if (r2 < r) { r2 = r; cur_end2 = cur_end; cur_del2 = cur_del; }
+            while (t2 >= cur_end2) { ++r2; cur_end2 = sm_end[r2]; cur_del2 = sm_del[r2]; }
+            const Atom<T> a1 = load_atom<T, GAS>(kp, t + cur_del);
+            const Atom<T> a2 = load_atom<T, GAS>(kp, t2 + cur_del2);
+            visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
+            visit_atom<T, GAS, HASQ>(kp, p, act, a2, acc);
+            r = r2; cur_end = cur_end2; cur_del = cur_del2;
+          }
+          if (t < total) {
+            while (t >= cur_end) { ++r; cur_end = sm_end[r]; cur_del = sm_del[r]; }
+            const Atom<T> a1 = load_atom<T, GAS>(kp, t + cur_del);
+            visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
+          }
+          nvis += (uint32_t)total;
+        }
+        __syncthreads();
+      }
+    }
+  }
+  // two-level reduction in a fixed order
+  T v[NV];
+#pragma unroll
+  for (int s = 0; s < NS; s++) {
+    v[4 * s] = acc.f[s][0]; v[4 * s + 1] = acc.f[s][1]; v[4 * s + 2] = acc.f[s][2]; v[4 * s + 3] = acc.U[s];
+  }
+#pragma unroll
+  for (int k = 0; k < 3; k++) v[4 * NS + k] = acc.E[k];
+#pragma unroll
+  for (int k = 0; k < 6; k++) v[4 * NS + 3 + k] = acc.G[k];
+#pragma unroll
+  for (int k = 0; k < NV; k++) v[k] = group_sum<32>(v[k], 0xffffffffu);
+  if constexpr (NW > 1) {
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < NV; k++) sm_red[w * NV + k] = v[k];
+    }
+    __syncthreads();
+    if (tid < NV) {  // one thread per value sums the warps in a fixed order
+      T sum = sm_red[tid];
+#pragma unroll
+      for (int q = 1; q < NW; q++) sum += sm_red[q * NV + tid];
+      sm_red[NW * NV + tid] = sum;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = sm_red[NW * NV + k];
+    __syncthreads();
+  }
+#pragma unroll
+  for (int s = 0; s < NS; s++) {
+    f[s][0] = v[4 * s]; f[s][1] = v[4 * s + 1]; f[s][2] = v[4 * s + 2]; U[s] = v[4 * s + 3];
+  }
+  if (HASQ && kp.dip_on) {
+    constexpr int d = GasShape<GAS>::DIP;
+    const T al = T(kp.alpha);
+    const T *E = v + 4 * NS, *Gr = v + 4 * NS + 3;
+    f[d][0] += al * (E[0] * Gr[0] + E[1] * Gr[3] + E[2] * Gr[4]);
+    f[d][1] += al * (E[0] * Gr[3] + E[1] * Gr[1] + E[2] * Gr[5]);
+    f[d][2] += al * (E[0] * Gr[4] + E[1] * Gr[5] + E[2] * Gr[2]);
+    U[d] -= T(0.5) * al * (E[0] * E[0] + E[1] * E[1] + E[2] * E[2]);
+  }
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+    if (!act[s]) { f[s][0] = f[s][1] = f[s][2] = U[s] = T(0); }
+  visits += nvis;
+}
+
 // ---- initial conditions: System::setup (System.cpp:1397-1518), FP64 -------
 __device__ __forceinline__ double vel_sample(const KParams &kp, double u) {
   // smallest k with S[k] >= u (the reference's linear scan, System.cpp:1549-1552)
@@ -381,7 +543,7 @@ struct Init {
   double pos[3][3], vel[3][3], rcm[3], vcm[3];
 };
 
-__device__ bool setup_probe(const KParams &kp, size_t j, Init &I) {
+__device__ __forceinline__ bool setup_probe(const KParams &kp, size_t j, Init &I) {
   const double *u = kp.rnd;
   const size_t st = kp.rnd_stride;
   double rcm[3] = {u[j], 0.0, kp.bmax};
@@ -422,14 +584,6 @@ __device__ bool setup_probe(const KParams &kp, size_t j, Init &I) {
   return true;
 }
 
-template <int G>
-__device__ __forceinline__ bool group_expired(const KParams &kp, int g, unsigned mask) {
-  int e = 0;
-  if (g == 0) e = global_ns() > kp.deadline_ns;
-  if constexpr (G > 1) e = __shfl_sync(mask, e, 0, G);
-  return e != 0;
-}
-
 // ---- shared integrator pieces -----------------------------------------------
 template <typename T> __device__ __forceinline__ T dot3(const T a[3], const T b[3]) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
@@ -466,303 +620,572 @@ __device__ __forceinline__ double one_minus_cos(const double vi[3], const T vf[3
 }
 template <typename T> __device__ __forceinline__ bool outside_box(const KParams &kp, const T r[3]) {
   if (fabs(r[0]) >= T(kp.lx) || fabs(r[1]) >= T(kp.ly) || fabs(r[2]) >= T(kp.lz)) return true;
-  const T ux = r[0] / T(kp.a), uy = r[1] / T(kp.b), uz = r[2] / T(kp.c);
+  const T ux = r[0] * T(kp.inv_a), uy = r[1] * T(kp.inv_b), uz = r[2] * T(kp.inv_c);
   return ux * ux + uy * uy + uz * uz > T(1);
 }
 
-struct TrajOut {
-  int8_t status;
-  double omc;
-  uint32_t steps, visits, calls;
+// ---- trajectory kernels ------------------------------------------------------
+// Two passes share one integrator (the step of run_He / run_N2 / run_CO2):
+//
+//  lane pass  every lane owns one trajectory; a warp advances 32 independent
+//             trajectories in SIMT.  The force phase is cooperative: lanes
+//             publish their site positions in shared memory, the lanes whose
+//             probe is within reach of the target are collected with a ballot,
+//             and subgroups of G lanes evaluate those probes (G = 1: every lane
+//             its own).  Probes out of reach feel exactly zero force.  A lane
+//             whose trajectory passes `park_steps` integration steps saves the
+//             exact integrator state to HBM ("parks" it) and takes new work.
+//  warp pass  parked trajectories resume one per warp: the force phase of a
+//             step uses all 32 lanes and the integrator runs warp-uniform, so
+//             the few very long trajectories (captured orbits with tens of
+//             thousands of steps) advance at the lowest per-step latency
+//             instead of sharing their warp with 31 others.
+//
+// Finished trajectories write status / 1-cos(chi) / steps / visits at their
+// own index.  Restarts rebuild the initial state from the trajectory's random
+// numbers (System::setup is deterministic), so no copy of the initial state is
+// kept.
+enum : int { M_IDLE = 0, M_INIT = 1, M_RESTART = 2, M_STEP = 3 };
+constexpr int BLOCK = 128;
+
+__device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
+  for (int k = 0; k < n; k++) m &= m - 1u;
+  return __ffs(m) - 1;
+}
+
+// Integrator state of one trajectory between force phases.  Atoms use
+// r1/v1/r1lo; molecules keep the constrained pair (r1, r2) and the pair forces
+// (f1, f2) of the last force phase; site positions are derived from it.
+template <typename T> struct LaneState {
+  T r1[3], r2[3], v1[3], v2[3], r1lo[3], r2lo[3];
+  T f1[3], f2[3];
+  T U, rold[3], dtheta, dt, Ei;
+  uint32_t stepcount, nsteps, nvis;
+  int tries, maxTries, mode;
+  unsigned long long j;
 };
 
-// ---- run_He (System.cpp:338-511): He, Ar, "co2" ------------------------------
-template <typename T, int G, bool HASQ>
-__device__ void run_atom(const KParams &kp, size_t j, int g, unsigned mask, int *sm_e, int *sm_d,
-                         TrajOut &o) {
-  Init I;
-  if (!setup_probe(kp, j, I)) { o.status = 0; return; }
-  const double vi64[3] = {I.vel[0][0], I.vel[0][1], I.vel[0][2]};
-  const T ri[3] = {T(I.pos[0][0]), T(I.pos[0][1]), T(I.pos[0][2])};
-  const T vi[3] = {T(vi64[0]), T(vi64[1]), T(vi64[2])};
-  const T mu = T(kp.mu), kconv = T(KCALMOLANGAMU_TO_ANGFS2), ke = T(AMUANGFS2_TO_KCAL_MOL);
-  T p[1][3], f[1][3], U[1], fi[3];
-  bool act[1];
-  for (int k = 0; k < 3; k++) p[0][k] = ri[k];
-  act[0] = ref_inside(kp, p[0][0], p[0][1], p[0][2]);
-  eval_forces<T, G, GAS_ATOM, HASQ>(kp, p, act, p[0], T(0), f, U, o.visits, g, mask, sm_e, sm_d);
-  o.calls++;
-  for (int k = 0; k < 3; k++) fi[k] = f[0][k];
-  const T Ei = U[0] + T(0.5) * mu * dot3(vi, vi) * ke;
-  const T theta_max = T(1.5 * PI_D);
-  T r[3], rlo[3], v[3], rold[3], dtheta = T(0);
-  T dt = T(kp.dt);
-  int tries = 0, maxTries = 8;
-  uint32_t stepcount = 0;
-  while (tries < maxTries && maxTries < 10) {
-    if (stepcount == 0) {
-      for (int k = 0; k < 3; k++) { r[k] = ri[k]; rlo[k] = T(0); v[k] = vi[k]; rold[k] = ri[k]; f[0][k] = fi[k]; }
-      dtheta = T(0);
-    }
-    const T kick = T(0.5) * dt / mu * kconv;
+template <int GAS> struct Sites {
+  static constexpr int NS = GasShape<GAS>::NS;
+  static constexpr int pa = 0, pb = GAS == GAS_CO2 ? 2 : 1, pc = GAS == GAS_CO2 ? 1 : 2;
+  static constexpr int cs = GAS == GAS_ATOM ? 0 : pc;  // reference point of the reach sphere
+};
+
+template <typename T, int GAS>
+__device__ __forceinline__ void site_positions(const LaneState<T> &L, T (&p)[GasShape<GAS>::NS][3]) {
+  using S = Sites<GAS>;
+  if constexpr (GAS == GAS_ATOM) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) p[0][k] = L.r1[k];
+  } else {
+#pragma unroll
     for (int k = 0; k < 3; k++) {
-      v[k] += kick * f[0][k];
-      // compensated position update (Kahan): r + rlo tracks the exact sum
-      const T y = dt * v[k] - rlo[k];
-      const T t = r[k] + y;
-      rlo[k] = (t - r[k]) - y;
-      r[k] = t;
-    }
-    dtheta += angle3(r, rold);
-    for (int k = 0; k < 3; k++) { rold[k] = r[k]; p[0][k] = r[k]; }
-    act[0] = ref_inside(kp, r[0], r[1], r[2]);
-    eval_forces<T, G, GAS_ATOM, HASQ>(kp, p, act, p[0], T(0), f, U, o.visits, g, mask, sm_e, sm_d);
-    o.calls++;
-    for (int k = 0; k < 3; k++) v[k] += kick * f[0][k];
-    stepcount++;
-    o.steps++;
-    if (dtheta > theta_max) {
-      tries++;
-      dt = T(kp.dt / (tries + 1));
-      stepcount = 0;
-      continue;
-    }
-    if (outside_box(kp, r)) {
-      const double E = (double)U[0] + (double)(T(0.5) * mu * dot3(v, v) * ke);
-      const double dE = fabs(E - (double)Ei) / (double)Ei * 100.0;
-      if (dE > kp.etol) {
-        tries++;
-        maxTries++;
-        dt = T(kp.dt / (tries + 1));
-        stepcount = 0;
-        continue;
-      }
-      o.status = 1;
-      o.omc = one_minus_cos<T>(vi64, v);
-      return;
-    }
-    if (stepcount >= kp.max_steps) { o.status = 3; return; }
-    if ((o.steps & 4095u) == 0 && group_expired<G>(kp, g, mask)) {
-      if (g == 0) atomicExch(kp.error, 1);
-      o.status = 3;
-      return;
+      p[S::pa][k] = L.r1[k];
+      p[S::pb][k] = L.r2[k];
+      p[S::pc][k] = T(0.5) * (L.r1[k] + L.r2[k]);
     }
   }
-  o.status = 2;
 }
 
-// ---- run_N2 (System.cpp:514-945) and run_CO2 (System.cpp:948-1392) ----------
-template <typename T, int G, int GAS, bool HASQ>
-__device__ void run_molecule(const KParams &kp, size_t j, int g, unsigned mask, int *sm_e,
-                             int *sm_d, TrajOut &o) {
-  constexpr bool co2 = GAS == GAS_CO2;
-  constexpr int pa = 0, pb = co2 ? 2 : 1, pc = co2 ? 1 : 2;
-  Init I;
-  if (!setup_probe(kp, j, I)) { o.status = 0; return; }
-  double vcm_i[3] = {I.vcm[0], I.vcm[1], I.vcm[2]};
-  if (co2 && (kp.quirks & 1)) vcm_i[0] = I.vcm[1];  // System.cpp:1012
-  const T ma = T(kp.gas_m[pa]), mb = T(kp.gas_m[pb]), mc = T(kp.gas_m[pc]), M = T(kp.gas_mass);
-  const T kconv = T(KCALMOLANGAMU_TO_ANGFS2), ke = T(AMUANGFS2_TO_KCAL_MOL);
-  const T d2 = T(kp.d_bond * kp.d_bond), theta_max = T(1.5 * PI_D);
-  T ri[3], rj[3], vi[3], vj[3], fg[3][3], Ug[3], pos[3][3], rold[3], rilo[3], rjlo[3];
-  bool act[3];
-  T Ei = T(0), dtheta = T(0), dt = T(kp.dt);
-  int tries = 0, maxTries = 8;
-  uint32_t stepcount = 0;
-  bool first = true;
-  while (tries < maxTries && maxTries < 10) {
-    if (stepcount == 0) {
-      // restart from the initial conditions (recomputed: identical bits every time)
-      if (!first) setup_probe(kp, j, I);
-      for (int s = 0; s < 3; s++)
-        for (int k = 0; k < 3; k++) pos[s][k] = T(I.pos[s][k]);
-      for (int k = 0; k < 3; k++) {
-        ri[k] = pos[pa][k]; rj[k] = pos[pb][k]; rilo[k] = rjlo[k] = T(0);
-        vi[k] = T(I.vel[pa][k]); vj[k] = T(I.vel[pb][k]); rold[k] = T(I.rcm[k]);
-      }
-      for (int s = 0; s < 3; s++) act[s] = kp.allpairs || ref_inside(kp, pos[s][0], pos[s][1], pos[s][2]);
-      const T cen[3] = {pos[pc][0], pos[pc][1], pos[pc][2]};
-      eval_forces<T, G, GAS, HASQ>(kp, pos, act, cen, T(0.5) * T(kp.d_bond), fg, Ug, o.visits, g,
-                                   mask, sm_e, sm_d);
-      o.calls += 3;
-      if (first) {
-        // initial energy: every site's kinetic energy (System.cpp:648-660, 1076-1088)
-        T ek = T(0);
-        for (int s = 0; s < 3; s++) {
-          const T vs[3] = {T(I.vel[s][0]), T(I.vel[s][1]), T(I.vel[s][2])};
-          ek += T(0.5) * T(kp.gas_m[s]) * dot3(vs, vs) * ke;
-        }
-        Ei = Ug[0] + Ug[1] + Ug[2] + ek;
-        first = false;
-      }
-      dtheta = T(0);
-    }
-    // pair forces: N2 splits the central charge half/half (System.cpp:736-739);
-    // CO2 redistributes the carbon force (Ciccotti, System.cpp:1154-1158)
-    T fi[3], fj[3];
-    if constexpr (co2) {
-      const T m2M = mc / M, m0M = ma / M;
-      for (int k = 0; k < 3; k++) {
-        fi[k] = (T(1) - T(0.5) * m2M) * fg[0][k] + m0M * fg[1][k] - T(0.5) * m2M * fg[2][k];
-        fj[k] = (T(1) - T(0.5) * m2M) * fg[2][k] + m0M * fg[1][k] - T(0.5) * m2M * fg[0][k];
-      }
-    } else {
-      for (int k = 0; k < 3; k++) { fi[k] = fg[0][k] + T(0.5) * fg[2][k]; fj[k] = fg[1][k] + T(0.5) * fg[2][k]; }
-    }
-    // first half of the constrained Verlet (System.cpp:1700-1739)
-    {
-      const T mu_ij = ma * mb / (ma + mb);
-      T vci[3], vcj[3], rij[3], rcij[3];
-      for (int k = 0; k < 3; k++) {
-        vci[k] = vi[k] + T(0.5) * dt / ma * fi[k] * kconv;
-        vcj[k] = vj[k] + T(0.5) * dt / mb * fj[k] * kconv;
-        rij[k] = ri[k] - rj[k];
-        rcij[k] = rij[k] + dt * (vci[k] - vcj[k]);
-      }
-      const T r2ij = dot3(rij, rij), rc2ij = dot3(rcij, rcij), rr = dot3(rcij, rij);
-      T det = rr * rr - r2ij * (rc2ij - d2);
-      if (det < T(0)) det = T(0);
-      const T lam = (rr - Real<T>::sq(det)) / r2ij;
-      const T ca = mu_ij / ma * lam, cb = mu_ij / ma * lam;  // the reference uses mi twice (:1735-1736)
-      for (int k = 0; k < 3; k++) {
-        vi[k] = vci[k] - mu_ij / (ma * dt) * lam * rij[k];
-        vj[k] = vcj[k] + mu_ij / (mb * dt) * lam * rij[k];
-        // compensated position updates
-        T y = (dt * vci[k] - ca * rij[k]) - rilo[k];
-        T t = ri[k] + y;
-        rilo[k] = (t - ri[k]) - y;
-        ri[k] = t;
-        y = (dt * vcj[k] + cb * rij[k]) - rjlo[k];
-        t = rj[k] + y;
-        rjlo[k] = (t - rj[k]) - y;
-        rj[k] = t;
-      }
-    }
-    T rcm[3], vcm[3];
-    for (int k = 0; k < 3; k++) { rcm[k] = T(0.5) * (ri[k] + rj[k]); vcm[k] = T(0.5) * (vi[k] + vj[k]); }
-    dtheta += angle3(rcm, rold);
-    for (int k = 0; k < 3; k++) {
-      rold[k] = rcm[k];
-      pos[pa][k] = ri[k]; pos[pb][k] = rj[k]; pos[pc][k] = rcm[k];
-    }
-    for (int s = 0; s < 3; s++) act[s] = kp.allpairs || ref_inside(kp, pos[s][0], pos[s][1], pos[s][2]);
-    {
-      T hd[3] = {ri[0] - rj[0], ri[1] - rj[1], ri[2] - rj[2]};
-      const T off = T(0.5) * Real<T>::sq(dot3(hd, hd));
-      eval_forces<T, G, GAS, HASQ>(kp, pos, act, rcm, off, fg, Ug, o.visits, g, mask, sm_e, sm_d);
-      o.calls += 3;
-    }
-    if constexpr (co2) {
-      const T m2M = mc / M, m0M = ma / M;
-      for (int k = 0; k < 3; k++) {
-        fi[k] = (T(1) - T(0.5) * m2M) * fg[0][k] + m0M * fg[1][k] - T(0.5) * m2M * fg[2][k];
-        fj[k] = (T(1) - T(0.5) * m2M) * fg[2][k] + m0M * fg[1][k] - T(0.5) * m2M * fg[0][k];
-      }
-    } else {
-      for (int k = 0; k < 3; k++) { fi[k] = fg[0][k] + T(0.5) * fg[2][k]; fj[k] = fg[1][k] + T(0.5) * fg[2][k]; }
-    }
-    // second half (RATTLE velocity correction, System.cpp:1741-1767)
-    {
-      const T mu_ij = ma * mb / (ma + mb);
-      T vci[3], vcj[3], rij[3], vcij[3];
-      for (int k = 0; k < 3; k++) {
-        vci[k] = vi[k] + T(0.5) * dt / ma * fi[k] * kconv;
-        vcj[k] = vj[k] + T(0.5) * dt / mb * fj[k] * kconv;
-        rij[k] = ri[k] - rj[k];
-        vcij[k] = vci[k] - vcj[k];
-      }
-      const T lam = mu_ij * dot3(rij, vcij) / dot3(rij, rij);
-      for (int k = 0; k < 3; k++) { vi[k] = vci[k] - lam / ma * rij[k]; vj[k] = vcj[k] + lam / mb * rij[k]; }
-    }
-    for (int k = 0; k < 3; k++) vcm[k] = T(0.5) * (vi[k] + vj[k]);
-    stepcount++;
-    o.steps++;
-    if (dtheta > theta_max) {
-      tries++;
-      dt = T(kp.dt / (tries + 1));
-      stepcount = 0;
-      continue;
-    }
-    if (outside_box(kp, rcm)) {
-      // N2: kinetic energy of the two N atoms (System.cpp:890-896);
-      // CO2: all three sites, the carbon moving with the centre (System.cpp:1333-1339)
-      T ek = T(0.5) * ma * dot3(vi, vi) * ke + T(0.5) * mb * dot3(vj, vj) * ke;
-      if (co2) ek += T(0.5) * mc * dot3(vcm, vcm) * ke;
-      const double E = (double)Ug[0] + (double)Ug[1] + (double)Ug[2] + (double)ek;
-      const double dE = fabs((E - (double)Ei) / (double)Ei) * 100.0;
-      if (dE > kp.etol) {
-        tries++;
-        maxTries++;
-        dt = T(kp.dt / (tries + 1));
-        stepcount = 0;
-        continue;
-      }
-      o.status = 1;
-      o.omc = one_minus_cos<T>(vcm_i, vcm);
-      return;
-    }
-    if (stepcount >= kp.max_steps) { o.status = 3; return; }
-    if ((o.steps & 4095u) == 0 && group_expired<G>(kp, g, mask)) {
-      if (g == 0) atomicExch(kp.error, 1);
-      o.status = 3;
-      return;
-    }
+// half the pair distance: how far a site can sit from the reference point
+template <typename T, int GAS>
+__device__ __forceinline__ T site_offset(const T (&p)[GasShape<GAS>::NS][3]) {
+  if constexpr (GAS == GAS_ATOM) {
+    return T(0);
+  } else {
+    using S = Sites<GAS>;
+    const T hd[3] = {p[S::pa][0] - p[S::pb][0], p[S::pa][1] - p[S::pb][1], p[S::pa][2] - p[S::pb][2]};
+    return T(0.5) * Real<T>::sq(dot3(hd, hd));
   }
-  o.status = 2;
 }
 
-// ---- the persistent trajectory kernel ----------------------------------------
-constexpr int MAX_BLOCK = 256;
+// the reach test (bounding box of the target) and the reference's grid rule
+template <typename T, int GAS>
+__device__ __forceinline__ bool probe_near(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
+                                           unsigned &actbits) {
+  using S = Sites<GAS>;
+  actbits = 0;
+#pragma unroll
+  for (int s = 0; s < S::NS; s++)
+    if (ref_inside(kp, p[s][0], p[s][1], p[s][2])) actbits |= 1u << s;
+  const T R = (kp.allpairs ? T(INFINITY) : T(kp.reach) + T(1e-3)) + site_offset<T, GAS>(p);
+  const T ex = fmax(fmax(T(kp.bb_lo[0]) - p[S::cs][0], p[S::cs][0] - T(kp.bb_hi[0])), T(0));
+  const T ey = fmax(fmax(T(kp.bb_lo[1]) - p[S::cs][1], p[S::cs][1] - T(kp.bb_hi[1])), T(0));
+  const T ez = fmax(fmax(T(kp.bb_lo[2]) - p[S::cs][2], p[S::cs][2] - T(kp.bb_hi[2])), T(0));
+  return actbits != 0 && ex * ex + ey * ey + ez * ez <= R * R;
+}
+
+// pair forces from the site forces: N2 splits the central charge half/half
+// (System.cpp:736-739); CO2 redistributes the carbon force (Ciccotti,
+// System.cpp:1154-1158); an atom keeps its own force.  Also sums U.
+template <typename T, int GAS>
+__device__ __forceinline__ void absorb_forces(const KParams &kp, const T (&fs)[GasShape<GAS>::NS][3],
+                                              const T (&Us)[GasShape<GAS>::NS], LaneState<T> &L) {
+  T u = T(0);
+#pragma unroll
+  for (int s = 0; s < GasShape<GAS>::NS; s++) u += Us[s];
+  L.U = u;
+  if constexpr (GAS == GAS_CO2) {
+    const T M = T(kp.gas_mass), m2M = T(kp.gas_m[1]) / M, m0M = T(kp.gas_m[0]) / M;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      L.f1[k] = (T(1) - T(0.5) * m2M) * fs[0][k] + m0M * fs[1][k] - T(0.5) * m2M * fs[2][k];
+      L.f2[k] = (T(1) - T(0.5) * m2M) * fs[2][k] + m0M * fs[1][k] - T(0.5) * m2M * fs[0][k];
+    }
+  } else if constexpr (GAS == GAS_N2) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      L.f1[k] = fs[0][k] + T(0.5) * fs[2][k];
+      L.f2[k] = fs[1][k] + T(0.5) * fs[2][k];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 3; k++) L.f1[k] = fs[0][k];
+  }
+}
+
+// Initial state of a trajectory (System::setup) and the initial kinetic
+// energy of every site (System.cpp:376-383, 648-660, 1076-1088).  Not inlined
+// (it runs once per trajectory and per retry); it returns by value so the
+// caller's integrator state never needs an address and stays in registers.
+template <typename T> struct InitState {
+  T r1[3], r2[3], v1[3], v2[3], rcm[3], ek;
+  int hit;
+};
+
+template <typename T, int GAS>
+__device__ __noinline__ InitState<T> lane_setup(const KParams *__restrict__ kpg, unsigned long long j) {
+  const KParams &kp = *kpg;
+  constexpr bool MOL = GAS != GAS_ATOM;
+  using S = Sites<GAS>;
+  InitState<T> o;
+  Init I;
+  o.hit = setup_probe(kp, (size_t)j, I) ? 1 : 0;
+  for (int k = 0; k < 3; k++) {
+    o.r1[k] = T(I.pos[S::pa][k]); o.v1[k] = T(I.vel[S::pa][k]);
+    o.r2[k] = T(I.pos[S::pb][k]); o.v2[k] = T(I.vel[S::pb][k]);
+    o.rcm[k] = T(I.rcm[k]);
+  }
+  T e = T(0);
+  for (int s = 0; s < (MOL ? 3 : 1); s++) {
+    const T vs[3] = {T(I.vel[s][0]), T(I.vel[s][1]), T(I.vel[s][2])};
+    e += T(0.5) * T(MOL ? kp.gas_m[s] : kp.mu) * dot3(vs, vs) * T(AMUANGFS2_TO_KCAL_MOL);
+  }
+  o.ek = e;
+  return o;
+}
+
+template <typename T, int GAS>
+__device__ __forceinline__ void load_init(LaneState<T> &L, const InitState<T> &I) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    L.r1[k] = I.r1[k]; L.v1[k] = I.v1[k]; L.r1lo[k] = T(0);
+    if constexpr (GAS != GAS_ATOM) { L.r2[k] = I.r2[k]; L.v2[k] = I.v2[k]; L.r2lo[k] = T(0); }
+    L.rold[k] = I.rcm[k];
+  }
+  L.dtheta = T(0);
+  L.stepcount = 0;
+}
+
+// 1 - cos(chi) against the initial centre-of-mass velocity, rebuilt in FP64
+// from the trajectory's random numbers.
+template <typename T, int GAS>
+__device__ __noinline__ double lane_chi(const KParams *__restrict__ kpg, unsigned long long j, T vx, T vy, T vz) {
+  const KParams &kp = *kpg;
+  Init I;
+  setup_probe(kp, (size_t)j, I);
+  double vref[3];
+  if constexpr (GAS == GAS_ATOM) {
+    for (int k = 0; k < 3; k++) vref[k] = I.vel[0][k];
+  } else {
+    for (int k = 0; k < 3; k++) vref[k] = I.vcm[k];
+    if (GAS == GAS_CO2 && (kp.quirks & 1)) vref[0] = I.vcm[1];  // System.cpp:1012
+  }
+  const T vf[3] = {vx, vy, vz};
+  return one_minus_cos<T>(vref, vf);
+}
+
+// First half of a step: kick, drift (constrained for molecules), angle.
+template <typename T, int GAS>
+__device__ __forceinline__ void first_half(const KParams &kp, LaneState<T> &L) {
+  using S = Sites<GAS>;
+  const T dt = L.dt, kconv = T(KCALMOLANGAMU_TO_ANGFS2);
+  if constexpr (GAS == GAS_ATOM) {
+    const T kick = dt * T(kp.half_kconv_over_m1);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      L.v1[k] += kick * L.f1[k];
+      const T y = dt * L.v1[k] - L.r1lo[k];  // compensated position update
+      const T t = L.r1[k] + y;
+      L.r1lo[k] = (t - L.r1[k]) - y;
+      L.r1[k] = t;
+    }
+    L.dtheta += angle3(L.r1, L.rold);
+#pragma unroll
+    for (int k = 0; k < 3; k++) L.rold[k] = L.r1[k];
+  } else {
+    // constrained Verlet, first half (System.cpp:1700-1739)
+    const T d2 = T(kp.d_bond * kp.d_bond);
+    const T ka = dt * T(kp.half_kconv_over_m1), kb = dt * T(kp.half_kconv_over_m2);
+    T vci[3], vcj[3], rij[3], rcij[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      vci[k] = L.v1[k] + ka * L.f1[k];
+      vcj[k] = L.v2[k] + kb * L.f2[k];
+      rij[k] = L.r1[k] - L.r2[k];
+      rcij[k] = rij[k] + dt * (vci[k] - vcj[k]);
+    }
+    const T r2ij = dot3(rij, rij), rc2ij = dot3(rcij, rcij), rr = dot3(rcij, rij);
+    T det = rr * rr - r2ij * (rc2ij - d2);
+    if (det < T(0)) det = T(0);
+    const T lam = Real<T>::div(rr - Real<T>::sq(det), r2ij);
+    const T cpos = T(kp.mu12_over_m1) * lam;  // the reference uses mi for both atoms (:1735-1736)
+    const T inv_dt = Real<T>::div(T(1), dt);
+    const T ca = cpos * inv_dt, cb = T(kp.mu12_over_m2) * lam * inv_dt;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      L.v1[k] = vci[k] - ca * rij[k];
+      L.v2[k] = vcj[k] + cb * rij[k];
+      T y = (dt * vci[k] - cpos * rij[k]) - L.r1lo[k];
+      T t = L.r1[k] + y;
+      L.r1lo[k] = (t - L.r1[k]) - y;
+      L.r1[k] = t;
+      y = (dt * vcj[k] + cpos * rij[k]) - L.r2lo[k];
+      t = L.r2[k] + y;
+      L.r2lo[k] = (t - L.r2[k]) - y;
+      L.r2[k] = t;
+    }
+    T rcm[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) rcm[k] = T(0.5) * (L.r1[k] + L.r2[k]);
+    L.dtheta += angle3(rcm, L.rold);
+#pragma unroll
+    for (int k = 0; k < 3; k++) L.rold[k] = rcm[k];
+  }
+}
+
+enum : int { S_CONTINUE = 0, S_RETRY_ANGLE = 1, S_RETRY_ENERGY = 2, S_SCATTER = 3, S_CAPPED = 4 };
+
+// Second half of a step and the exit tests (System.cpp:441-506, 835-940,
+// 1268-1387).  vc receives the centre-of-mass velocity for chi.
+template <typename T, int GAS>
+__device__ __forceinline__ int second_half(const KParams &kp, LaneState<T> &L, T vc[3]) {
+  using S = Sites<GAS>;
+  const T dt = L.dt, kconv = T(KCALMOLANGAMU_TO_ANGFS2), ke = T(AMUANGFS2_TO_KCAL_MOL);
+  T rc[3], ek;
+  if constexpr (GAS == GAS_ATOM) {
+    const T kick = dt * T(kp.half_kconv_over_m1);
+#pragma unroll
+    for (int k = 0; k < 3; k++) { L.v1[k] += kick * L.f1[k]; vc[k] = L.v1[k]; rc[k] = L.r1[k]; }
+    ek = T(0.5) * T(kp.mu) * dot3(L.v1, L.v1) * ke;
+  } else {
+    // RATTLE velocity correction (System.cpp:1741-1767)
+    const T ma = T(kp.gas_m[S::pa]), mb = T(kp.gas_m[S::pb]);
+    const T ka = dt * T(kp.half_kconv_over_m1), kb = dt * T(kp.half_kconv_over_m2);
+    T vci[3], vcj[3], rij[3], vcij[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      vci[k] = L.v1[k] + ka * L.f1[k];
+      vcj[k] = L.v2[k] + kb * L.f2[k];
+      rij[k] = L.r1[k] - L.r2[k];
+      vcij[k] = vci[k] - vcj[k];
+    }
+    const T lam = Real<T>::div(T(kp.mu12) * dot3(rij, vcij), dot3(rij, rij));
+    const T la = lam * T(kp.inv_m1), lb = lam * T(kp.inv_m2);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      L.v1[k] = vci[k] - la * rij[k];
+      L.v2[k] = vcj[k] + lb * rij[k];
+      vc[k] = T(0.5) * (L.v1[k] + L.v2[k]);
+      rc[k] = T(0.5) * (L.r1[k] + L.r2[k]);
+    }
+    // N2: the two N atoms (System.cpp:890-896); CO2: all sites, carbon at vcm (:1333-1339)
+    ek = T(0.5) * ma * dot3(L.v1, L.v1) * ke + T(0.5) * mb * dot3(L.v2, L.v2) * ke;
+    if (GAS == GAS_CO2) ek += T(0.5) * T(kp.gas_m[S::pc]) * dot3(vc, vc) * ke;
+  }
+  L.stepcount++;
+  L.nsteps++;
+  if (L.dtheta > T(1.5 * PI_D)) return S_RETRY_ANGLE;
+  if (outside_box(kp, rc)) {
+    const double E = (double)L.U + (double)ek;
+    const double dE = fabs((E - (double)L.Ei) / (double)L.Ei) * 100.0;
+    return dE > kp.etol ? S_RETRY_ENERGY : S_SCATTER;
+  }
+  return L.stepcount >= kp.max_steps ? S_CAPPED : S_CONTINUE;
+}
+
+// Result of one trajectory.
+template <typename T>
+__device__ __forceinline__ void write_result(const KParams &kp, const LaneState<T> &L, int8_t st, double omc,
+                                             unsigned long long *blk) {
+  kp.status[L.j] = st;
+  kp.omc[L.j] = st == 1 ? omc : 0.0;
+  if (kp.steps) kp.steps[L.j] = L.nsteps;
+  if (kp.visits) kp.visits[L.j] = L.nvis;
+  atomicAdd(&blk[st], 1ull);
+  atomicAdd(&blk[4], (unsigned long long)L.nsteps);
+  atomicAdd(&blk[5], (unsigned long long)L.nvis);
+}
 
 template <typename T, int G, int GAS, bool HASQ>
-__global__ void __launch_bounds__(MAX_BLOCK) traj_kernel(KParams kp) {
-  __shared__ int sm_end[MAX_BLOCK], sm_del[MAX_BLOCK];
-  __shared__ unsigned long long blk[7];
-  if (threadIdx.x < 7) blk[threadIdx.x] = 0ull;
+__global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParams *__restrict__ kpg) {
+  using S = Sites<GAS>;
+  constexpr int NS = S::NS;
+  constexpr int NSUB = 32 / G;
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ T sm_pos[BLOCK][NS][3];
+  __shared__ T sm_res[BLOCK][NS][4];
+  __shared__ uint32_t sm_vis[BLOCK];
+  __shared__ unsigned sm_act[BLOCK];
+  __shared__ int sm_end[BLOCK], sm_del[BLOCK];
+  __shared__ unsigned long long blk[8];
+  if (threadIdx.x < 8) blk[threadIdx.x] = 0ull;
   __syncthreads();
+
   const int lane = threadIdx.x & 31;
+  const int wbase = threadIdx.x & ~31;
   const int g = lane & (G - 1);
-  const unsigned mask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
-  int *sme = sm_end + (threadIdx.x & ~(G - 1));
-  int *smd = sm_del + (threadIdx.x & ~(G - 1));
-  unsigned long long cnt[7] = {0, 0, 0, 0, 0, 0, 0};
+  const int sub = lane / G;
+  const unsigned gmask = G == 32 ? FULL : (((1u << G) - 1u) << (sub * G));
+
+  LaneState<T> L;
+  L.mode = M_IDLE;
+
+  // take trajectories until one hits the ellipsoid (misses are written as free)
+  auto grab = [&]() {
+    for (;;) {
+      const unsigned long long jj = atomicAdd(kp.work, 1ull);
+      if (jj >= kp.ntraj || *(volatile int *)kp.error) { L.mode = M_IDLE; return; }
+      L.j = kp.order ? (unsigned long long)__ldg(&kp.order[jj]) : jj;
+      L.nsteps = 0;
+      L.nvis = 0;
+      const InitState<T> I = lane_setup<T, GAS>(kpg, L.j);
+      if (!I.hit) { write_result(kp, L, 0, 0.0, blk); continue; }
+      load_init<T, GAS>(L, I);
+      L.Ei = I.ek;  // completed with the initial potential energy by the first force phase
+      L.tries = 0;
+      L.maxTries = 8;
+      L.dt = T(kp.dt);
+      L.mode = M_INIT;
+      return;
+    }
+  };
+
+  grab();
+  unsigned it = 0;
   for (;;) {
-    // lane 0 takes the next trajectory (or stops the group after a watchdog
-    // expiry); the decision is broadcast so the whole group leaves together
-    unsigned long long jj = 0;
-    if (g == 0) jj = *(volatile int *)kp.error ? kp.ntraj : atomicAdd(kp.work, 1ull);
-    if constexpr (G > 1) jj = __shfl_sync(mask, jj, 0, G);
-    if (jj >= kp.ntraj) break;
-    const size_t j = (size_t)jj;
-    TrajOut o{0, 0.0, 0u, 0u, 0u};
-    if constexpr (GAS == GAS_ATOM) run_atom<T, G, HASQ>(kp, j, g, mask, sme, smd, o);
-    else run_molecule<T, G, GAS, HASQ>(kp, j, g, mask, sme, smd, o);
-    if (g == 0) {
-      kp.status[j] = o.status;
-      kp.omc[j] = o.status == 1 ? o.omc : 0.0;
-      if (kp.steps) kp.steps[j] = o.steps;
-      if (kp.visits) kp.visits[j] = o.visits;
-      cnt[o.status < 4 ? o.status : 3]++;
-      cnt[4] += o.steps;
-      cnt[5] += o.visits;
-      cnt[6] += o.calls;
+    if ((++it & 127u) == 0) {  // watchdog, one answer per warp
+      int e = 0;
+      if (lane == 0) e = global_ns() > kp.deadline_ns || *(volatile int *)kp.error;
+      e = __shfl_sync(FULL, e, 0);
+      if (e) {
+        if (lane == 0) atomicExch(kp.error, 1);
+        if (L.mode != M_IDLE) write_result(kp, L, 3, 0.0, blk);
+        L.mode = M_IDLE;
+      }
+    }
+    if (__all_sync(FULL, L.mode == M_IDLE)) break;
+
+    if (L.mode == M_STEP) first_half<T, GAS>(kp, L);
+
+    // ---- force phase
+    bool near = false;
+    unsigned actbits = 0;
+    T fs[NS][3], Us[NS];
+    if (L.mode != M_IDLE) {
+      T p[NS][3];
+      site_positions<T, GAS>(L, p);
+      near = probe_near<T, GAS>(kp, p, actbits);
+      if (near) {
+        if constexpr (G == 1) {
+          bool act[NS];
+#pragma unroll
+          for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
+          eval_forces<T, 1, GAS, HASQ>(kp, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis, 0,
+                                       1u << lane, nullptr, nullptr);
+        } else {
+#pragma unroll
+          for (int s = 0; s < NS; s++)
+#pragma unroll
+            for (int k = 0; k < 3; k++) sm_pos[threadIdx.x][s][k] = p[s][k];
+          sm_act[threadIdx.x] = actbits;
+        }
+      }
+    }
+    if constexpr (G > 1) {
+      __syncwarp();
+      const unsigned bal = __ballot_sync(FULL, near);
+      const int nn = __popc(bal);
+      for (int idx = sub; idx < nn; idx += NSUB) {
+        const int t = wbase + nth_set_bit(bal, idx);
+        T P[NS][3], ff[NS][3], UU[NS];
+        bool act[NS];
+        const unsigned ab = sm_act[t];
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+          act[s] = (ab >> s) & 1u;
+#pragma unroll
+          for (int k = 0; k < 3; k++) P[s][k] = sm_pos[t][s][k];
+        }
+        uint32_t nv = 0;
+        eval_forces<T, G, GAS, HASQ>(kp, P, act, P[S::cs], site_offset<T, GAS>(P), ff, UU, nv, g, gmask,
+                                     sm_end + wbase + sub * G, sm_del + wbase + sub * G);
+        if (g == 0) {
+#pragma unroll
+          for (int s = 0; s < NS; s++) {
+            sm_res[t][s][0] = ff[s][0]; sm_res[t][s][1] = ff[s][1];
+            sm_res[t][s][2] = ff[s][2]; sm_res[t][s][3] = UU[s];
+          }
+          sm_vis[t] = nv;
+        }
+      }
+      __syncwarp();
+      if (near) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+          fs[s][0] = sm_res[threadIdx.x][s][0]; fs[s][1] = sm_res[threadIdx.x][s][1];
+          fs[s][2] = sm_res[threadIdx.x][s][2]; Us[s] = sm_res[threadIdx.x][s][3];
+        }
+        L.nvis += sm_vis[threadIdx.x];
+      }
+    }
+    if (L.mode == M_IDLE) continue;
+    if (!near) {
+#pragma unroll
+      for (int s = 0; s < NS; s++) fs[s][0] = fs[s][1] = fs[s][2] = Us[s] = T(0);
+    }
+    absorb_forces<T, GAS>(kp, fs, Us, L);
+
+    // ---- second half, exit tests, retries, parking
+    if (L.mode == M_INIT) {
+      L.Ei += L.U;
+      L.mode = M_STEP;
+    } else if (L.mode == M_RESTART) {
+      L.mode = M_STEP;
+    } else {
+      T vc[3];
+      const int r = second_half<T, GAS>(kp, L, vc);
+      if (r == S_SCATTER) {
+        write_result(kp, L, 1, lane_chi<T, GAS>(kpg, L.j, vc[0], vc[1], vc[2]), blk);
+        grab();
+      } else if (r == S_CAPPED) {
+        write_result(kp, L, 3, 0.0, blk);
+        grab();
+      } else if (r != S_CONTINUE) {
+        // a failed try: smaller time step and a fresh start (System.cpp:453-458, 468-473)
+        L.tries++;
+        if (r == S_RETRY_ENERGY) L.maxTries++;
+        L.dt = T(kp.dt / (L.tries + 1));
+        if (!(L.tries < L.maxTries && L.maxTries < 10)) {
+          write_result(kp, L, 2, 0.0, blk);
+          grab();
+        } else {
+          load_init<T, GAS>(L, lane_setup<T, GAS>(kpg, L.j));
+          L.mode = M_RESTART;
+        }
+      } else if (kp.park && L.nsteps >= kp.park_steps) {
+        const unsigned long long slot = atomicAdd(kp.park_count, 1ull);
+        if (slot < kp.park_cap) {
+          reinterpret_cast<LaneState<T> *>(kp.park)[slot] = L;
+          atomicAdd(&blk[7], 1ull);
+          grab();
+        }
+      }
     }
   }
-  if (g == 0) {
-    for (int k = 0; k < 7; k++)
-      if (cnt[k]) atomicAdd(&blk[k], cnt[k]);
+  __syncthreads();
+  if (threadIdx.x < 6 && blk[threadIdx.x]) atomicAdd(&kp.stats[threadIdx.x], blk[threadIdx.x]);
+  if (threadIdx.x == 7 && blk[7]) atomicAdd(&kp.stats[6], blk[7]);
+}
+
+// Warp pass: parked trajectories resume one per CTA (all RBLOCK threads hold
+// the same state; the force phase is block-cooperative).
+constexpr int RBLOCK = 128;  // threads per trajectory in the warp pass
+
+template <typename T, int GAS, bool HASQ>
+__global__ void __launch_bounds__(RBLOCK) resume_kernel(KParams kp, const KParams *__restrict__ kpg) {
+  using S = Sites<GAS>;
+  constexpr int NS = S::NS;
+  constexpr int NV = 4 * NS + 9;
+  __shared__ int sm_end[RBLOCK], sm_del[RBLOCK], sm_wsum[RBLOCK / 32];
+  __shared__ T sm_red[(RBLOCK / 32 + 1) * NV];
+  __shared__ unsigned long long blk[8];
+  __shared__ unsigned long long sm_idx;
+  if (threadIdx.x < 8) blk[threadIdx.x] = 0ull;
+  __syncthreads();
+  const int tid = threadIdx.x;
+  unsigned long long np = *(volatile unsigned long long *)kp.park_count;
+  if (np > kp.park_cap) np = kp.park_cap;
+  for (;;) {
+    if (tid == 0) sm_idx = *(volatile int *)kp.error ? np : atomicAdd(kp.park_next, 1ull);
+    __syncthreads();
+    const unsigned long long idx = sm_idx;
+    __syncthreads();
+    if (idx >= np) break;
+    LaneState<T> L = reinterpret_cast<const LaneState<T> *>(kp.park)[idx];
+    for (unsigned it = 1;; it++) {
+      if ((it & 1023u) == 0) {
+        if (tid == 0) sm_idx = (global_ns() > kp.deadline_ns || *(volatile int *)kp.error) ? 1ull : 0ull;
+        __syncthreads();
+        const bool e = sm_idx != 0;
+        __syncthreads();
+        if (e) {
+          if (tid == 0) { atomicExch(kp.error, 1); write_result(kp, L, 3, 0.0, blk); }
+          break;
+        }
+      }
+      if (L.mode == M_STEP) first_half<T, GAS>(kp, L);
+      T p[NS][3], fs[NS][3], Us[NS];
+      site_positions<T, GAS>(L, p);
+      unsigned actbits;
+      if (probe_near<T, GAS>(kp, p, actbits)) {
+        bool act[NS];
+#pragma unroll
+        for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
+        eval_forces_block<T, RBLOCK, GAS, HASQ>(kp, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
+                                              tid, sm_end, sm_del, sm_wsum, sm_red);
+      } else {
+#pragma unroll
+        for (int s = 0; s < NS; s++) fs[s][0] = fs[s][1] = fs[s][2] = Us[s] = T(0);
+      }
+      absorb_forces<T, GAS>(kp, fs, Us, L);
+      if (L.mode == M_INIT) { L.Ei += L.U; L.mode = M_STEP; continue; }
+      if (L.mode == M_RESTART) { L.mode = M_STEP; continue; }
+      T vc[3];
+      const int r = second_half<T, GAS>(kp, L, vc);
+      if (r == S_CONTINUE) continue;
+      if (r == S_SCATTER) {
+        const double omc = lane_chi<T, GAS>(kpg, L.j, vc[0], vc[1], vc[2]);
+        if (tid == 0) write_result(kp, L, 1, omc, blk);
+        break;
+      }
+      if (r == S_CAPPED) {
+        if (tid == 0) write_result(kp, L, 3, 0.0, blk);
+        break;
+      }
+      L.tries++;
+      if (r == S_RETRY_ENERGY) L.maxTries++;
+      L.dt = T(kp.dt / (L.tries + 1));
+      if (!(L.tries < L.maxTries && L.maxTries < 10)) {
+        if (tid == 0) write_result(kp, L, 2, 0.0, blk);
+        break;
+      }
+      load_init<T, GAS>(L, lane_setup<T, GAS>(kpg, L.j));
+      L.mode = M_RESTART;
+    }
+    __syncthreads();
   }
   __syncthreads();
-  if (threadIdx.x < 7 && blk[threadIdx.x]) atomicAdd(&kp.stats[threadIdx.x], blk[threadIdx.x]);
+  if (threadIdx.x < 6 && blk[threadIdx.x]) atomicAdd(&kp.stats[threadIdx.x], blk[threadIdx.x]);
 }
 
 // Site-force evaluation at given points (ccs_eval_site_forces): one group per point.
 template <typename T, int G, int GAS, bool HASQ>
-__global__ void __launch_bounds__(MAX_BLOCK)
+__global__ void __launch_bounds__(BLOCK)
     force_points_kernel(KParams kp, int site, size_t npts, const double *pts, double *f, double *U,
                         uint32_t *vis) {
   constexpr int NS = GasShape<GAS>::NS;
-  __shared__ int sm_end[MAX_BLOCK], sm_del[MAX_BLOCK];
+  __shared__ int sm_end[BLOCK], sm_del[BLOCK];
   const int lane = threadIdx.x & 31;
   const int g = lane & (G - 1);
   const unsigned mask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
@@ -785,6 +1208,21 @@ __global__ void __launch_bounds__(MAX_BLOCK)
       if (vis) vis[i] = v;
     }
   }
+}
+
+// Expected-length key of every trajectory for longest-first scheduling:
+// the chord through the ellipsoid's bounding sphere over the sampled speed.
+// Slow probes with small impact parameters run longest (they are the ones
+// captured into orbits and retried); starting them first keeps the longest
+// serial chains off the end of the launch.  Only the order changes, never a result.
+__global__ void order_key_kernel(KParams kp, float *key, uint32_t *idx) {
+  const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= kp.ntraj) return;
+  const double v = vel_sample(kp, kp.rnd[kp.rnd_stride + j]);
+  const double b = kp.rnd[j] / kp.bmax;
+  const double chord = sqrt(fmax(1.0 - b * b, 0.01));
+  key[j] = (float)(chord / fmax(v, 1e-12));
+  idx[j] = (uint32_t)j;
 }
 
 // Initial conditions (ccs_eval_setup): one thread per trajectory.

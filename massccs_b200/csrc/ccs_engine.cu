@@ -18,6 +18,8 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "../../include/massccs_gpu.h"
 #include "ccs_device.cuh"
 
@@ -27,7 +29,7 @@ struct ccs_ctx {
   int device = 0;
   int sm_count = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev[6] = {};
+  cudaEvent_t ev[10] = {};  // [0..4] ccs_run, [5..7] passes, [8..9] autotuner
   ccs_params p{};
   bool have_params = false, have_target = false;
   std::string err;
@@ -44,7 +46,7 @@ struct ccs_ctx {
   double *d_vtab_v = nullptr, *d_vtab_s = nullptr;
   int vtab_n = 0;
   // per-run scratch
-  unsigned long long *d_work = nullptr;  // [0] work counter, [1..7] stats, [8] clock scratch
+  unsigned long long *d_work = nullptr;  // [0] work counter, [1..7] stats, [8] clock, [9] parked, [10] resumed
   int *d_error = nullptr;
   double *d_rnd = nullptr;
   size_t rnd_cap = 0;
@@ -52,6 +54,17 @@ struct ccs_ctx {
   double *d_omc = nullptr;
   uint32_t *d_steps = nullptr, *d_visits = nullptr;
   size_t out_cap = 0;
+  // longest-first processing order
+  float *d_key = nullptr, *d_key2 = nullptr;
+  uint32_t *d_idx = nullptr, *d_idx2 = nullptr;
+  void *d_sort_tmp = nullptr;
+  size_t order_cap = 0, sort_tmp_bytes = 0;
+  // parked long trajectories (lane pass -> warp pass)
+  void *d_park = nullptr;
+  size_t park_bytes = 0;
+  // device copy of the launch parameters (read by the non-inlined set-up code)
+  KParams *d_kparams = nullptr;
+  KParams h_kparams{};
   // launch choice
   int tuned_G = 0, tuned_block = 0;
   ccs_stats last{};
@@ -138,7 +151,8 @@ void vel_table(double m_amu, double T, std::vector<double> &V, std::vector<doubl
   }
 }
 
-using KernelFn = void (*)(KParams);
+using KernelFn = void (*)(KParams, const KParams *);
+template <typename T, int GAS, bool HASQ> KernelFn resume_ptr() { return resume_kernel<T, GAS, HASQ>; }
 using ForceFn = void (*)(KParams, int, size_t, const double *, double *, double *, uint32_t *);
 
 template <typename T, int G, int GAS, bool HASQ> KernelFn traj_ptr() { return traj_kernel<T, G, GAS, HASQ>; }
@@ -146,13 +160,12 @@ template <typename T, int G, int GAS, bool HASQ> ForceFn force_ptr() {
   return force_points_kernel<T, G, GAS, HASQ>;
 }
 
-constexpr int NG = 6;  // G = 1,2,4,8,16,32
 int g_index(int G) { int i = 0; while ((1 << i) < G) i++; return i; }
 
 template <typename T, int GAS, bool HASQ> KernelFn pick_traj_g(int gi) {
   switch (gi) {
     case 0: return traj_ptr<T, 1, GAS, HASQ>();
-    case 1: return traj_ptr<T, 2, GAS, HASQ>();
+    case 1:
     case 2: return traj_ptr<T, 4, GAS, HASQ>();
     case 3: return traj_ptr<T, 8, GAS, HASQ>();
     case 4: return traj_ptr<T, 16, GAS, HASQ>();
@@ -181,6 +194,18 @@ KernelFn pick_traj(const ccs_ctx *c, int G) {
   const bool hasq = c->coul_on || c->dip_on;
   return c->p.precision == CCS_PREC_FP64 ? pick_traj_t<double>(gas, hasq, g_index(G))
                                          : pick_traj_t<float>(gas, hasq, g_index(G));
+}
+KernelFn pick_resume(const ccs_ctx *c) {
+  const int gas = gas_kind(c->p.gas);
+  const bool hasq = c->coul_on || c->dip_on;
+  if (c->p.precision == CCS_PREC_FP64) {
+    if (gas == GAS_ATOM) return hasq ? resume_ptr<double, GAS_ATOM, true>() : resume_ptr<double, GAS_ATOM, false>();
+    if (gas == GAS_N2) return hasq ? resume_ptr<double, GAS_N2, true>() : resume_ptr<double, GAS_N2, false>();
+    return hasq ? resume_ptr<double, GAS_CO2, true>() : resume_ptr<double, GAS_CO2, false>();
+  }
+  if (gas == GAS_ATOM) return hasq ? resume_ptr<float, GAS_ATOM, true>() : resume_ptr<float, GAS_ATOM, false>();
+  if (gas == GAS_N2) return hasq ? resume_ptr<float, GAS_N2, true>() : resume_ptr<float, GAS_N2, false>();
+  return hasq ? resume_ptr<float, GAS_CO2, true>() : resume_ptr<float, GAS_CO2, false>();
 }
 ForceFn pick_force(const ccs_ctx *c, int G) {
   const int gas = gas_kind(c->p.gas);
@@ -225,6 +250,7 @@ KParams base_params(const ccs_ctx *c) {
   // reference grid: cells of lj_cutoff + skin over the box (LinkedCell.cpp:48-90)
   const double rh = p.lj_cutoff + p.skin;
   k.ref_h = rh;
+  k.ref_inv_h = 1.0 / rh;
   k.ref_nx = (int)std::ceil(2.0 * p.a / rh);
   k.ref_ny = (int)std::ceil(2.0 * p.b / rh);
   k.ref_nz = (int)std::ceil(2.0 * p.c / rh);
@@ -236,7 +262,21 @@ KParams base_params(const ccs_ctx *c) {
   k.dt = p.dt; k.mu = p.mu; k.temperature = p.temperature; k.gas_inertia = p.gas_inertia;
   k.d_bond = p.d_bond; k.a = p.a; k.b = p.b; k.c = p.c; k.bmax = p.bmax;
   k.lx = p.lx; k.ly = p.ly; k.lz = p.lz;
+  k.inv_a = 1.0 / p.a; k.inv_b = 1.0 / p.b; k.inv_c = 1.0 / p.c;
   k.etol = p.gas == CCS_GAS_N2 ? 1.0 : p.gas == CCS_GAS_CO2 ? 20.0 : 0.5;
+  {
+    // the moving pair: atoms integrate the reduced mass; N2 the two N; CO2 the two O
+    const double m1 = is_molecule(p.gas) ? gm[0] : p.mu;
+    const double m2 = is_molecule(p.gas) ? (p.gas == CCS_GAS_CO2 ? gm[2] : gm[1]) : p.mu;
+    const double kc = KCALMOLANGAMU_TO_ANGFS2;
+    k.half_kconv_over_m1 = 0.5 * kc / m1;
+    k.half_kconv_over_m2 = 0.5 * kc / m2;
+    k.inv_m1 = 1.0 / m1;
+    k.inv_m2 = 1.0 / m2;
+    k.mu12 = m1 * m2 / (m1 + m2);
+    k.mu12_over_m1 = k.mu12 / m1;
+    k.mu12_over_m2 = k.mu12 / m2;
+  }
   k.quirks = p.quirks;
   k.max_steps = p.max_steps_per_try ? p.max_steps_per_try : 2000000u;
   k.vtab_v = c->d_vtab_v; k.vtab_s = c->d_vtab_s; k.vtab_n = c->vtab_n;
@@ -301,14 +341,63 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, 0));
   if (per_sm < 1) per_sm = 1;
   size_t grid = (size_t)per_sm * c->sm_count;
-  const size_t max_useful = (n * (size_t)G + block - 1) / block;
+  const size_t max_useful = (n + block - 1) / block;  // one trajectory per lane
   if (grid > max_useful) grid = std::max<size_t>(1, max_useful);
   k.deadline_ns = now + (unsigned long long)(wd * 1e9);
-  // d_work: [0] work counter, [1..7] statistics, [8] clock scratch
+  // longest-expected-first processing order (a radix sort of the length keys)
+  if (n > 1 && c->p.schedule == 1) {
+    if (n > c->order_cap) {
+      dfree(c->d_key); dfree(c->d_key2); dfree(c->d_idx); dfree(c->d_idx2); dfree(c->d_sort_tmp);
+      c->order_cap = 0;
+      CK(cudaMalloc(&c->d_key, n * sizeof(float)));
+      CK(cudaMalloc(&c->d_key2, n * sizeof(float)));
+      CK(cudaMalloc(&c->d_idx, n * sizeof(uint32_t)));
+      CK(cudaMalloc(&c->d_idx2, n * sizeof(uint32_t)));
+      size_t tmp = 0;
+      CK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, c->d_key, c->d_key2, c->d_idx, c->d_idx2, (int)n));
+      CK(cudaMalloc(&c->d_sort_tmp, tmp));
+      c->sort_tmp_bytes = tmp;
+      c->order_cap = n;
+    }
+    order_key_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(k, c->d_key, c->d_idx);
+    CK(cudaGetLastError());
+    size_t tmp = c->sort_tmp_bytes;
+    CK(cub::DeviceRadixSort::SortPairsDescending(c->d_sort_tmp, tmp, c->d_key, c->d_key2, c->d_idx, c->d_idx2,
+                                                 (int)n, 0, 32, s));
+    k.order = c->d_idx2;
+  }
+  // parking buffer for trajectories that outlast park_steps in the lane pass
+  const size_t state_bytes = c->p.precision == CCS_PREC_FP64 ? sizeof(LaneState<double>) : sizeof(LaneState<float>);
+  const size_t cap = std::min<size_t>(n, std::max<size_t>(65536, n / 4));
+  if (cap * state_bytes > c->park_bytes) {
+    dfree(c->d_park);
+    c->park_bytes = 0;
+    CK(cudaMalloc(&c->d_park, cap * state_bytes));
+    c->park_bytes = cap * state_bytes;
+  }
+  k.park = c->d_park;
+  k.park_cap = cap;
+  k.park_steps = c->p.park_steps ? c->p.park_steps : 2048u;
+  k.park_count = c->d_work + 9;
+  k.park_next = c->d_work + 10;
+  // d_work: [0] work counter, [1..7] statistics, [8] clock scratch, [9] parked, [10] resumed
   CK(cudaMemsetAsync(c->d_work, 0, 8 * sizeof(unsigned long long), s));
+  CK(cudaMemsetAsync(c->d_work + 9, 0, 2 * sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(c->d_error, 0, sizeof(int), s));
-  fn<<<(unsigned)grid, block, 0, s>>>(k);
+  c->h_kparams = k;
+  CK(cudaMemcpyAsync(c->d_kparams, &c->h_kparams, sizeof(KParams), cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(c->ev[5], s));
+  fn<<<(unsigned)grid, block, 0, s>>>(k, c->d_kparams);
   CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[6], s));
+  // warp pass over the parked trajectories (exits at once when none were parked)
+  KernelFn rfn = pick_resume(c);
+  int rper_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, RBLOCK, 0));
+  if (rper_sm < 1) rper_sm = 1;
+  rfn<<<(unsigned)((size_t)rper_sm * c->sm_count), RBLOCK, 0, s>>>(k, c->d_kparams);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[7], s));
   c->last.grid_size = (int32_t)grid;
   c->last.block_size = block;
   c->last.lanes_per_traj = G;
@@ -318,12 +407,20 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
 int read_stats(ccs_ctx *c, ccs_stats *st, size_t n) {
   unsigned long long h[7];
   int herr = 0;
+  {
+    float a = 0, b = 0;
+    CK(cudaEventSynchronize(c->ev[7]));
+    CK(cudaEventElapsedTime(&a, c->ev[5], c->ev[6]));
+    CK(cudaEventElapsedTime(&b, c->ev[6], c->ev[7]));
+    c->last.lane_ms = a;
+    c->last.warp_ms = b;
+  }
   CK(cudaMemcpyAsync(h, c->d_work + 1, sizeof h, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(&herr, c->d_error, sizeof herr, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->last.ntraj = n;
   c->last.nfree = h[0]; c->last.nscatter = h[1]; c->last.nlost = h[2]; c->last.ncapped = h[3];
-  c->last.steps = h[4]; c->last.visits = h[5]; c->last.force_calls = h[6];
+  c->last.steps = h[4]; c->last.visits = h[5]; c->last.parked = h[6];
   if (st) *st = c->last;
   if (herr) return fail(c, CCS_ERR_TIMEOUT, "device watchdog expired after %.0f s",
                         c->p.watchdog_s > 0 ? c->p.watchdog_s : 600.0);
@@ -335,20 +432,20 @@ int read_stats(ccs_ctx *c, ccs_stats *st, size_t n) {
 int autotune(ccs_ctx *c, size_t n, size_t stride, int block) {
   if (c->p.lanes_per_traj > 0) { c->tuned_G = c->p.lanes_per_traj; c->tuned_block = block; return CCS_OK; }
   if (c->tuned_G) return CCS_OK;
-  const int cand[4] = {1, 4, 8, 32};
-  size_t slice = std::min<size_t>(n, (size_t)c->sm_count * 64);
+  const int cand[4] = {1, 8, 16, 32};
+  size_t slice = std::min<size_t>(n, (size_t)c->sm_count * 256);
   float best = 1e30f;
   int bestG = 32;
   for (int G : cand) {
     for (int rep = 0; rep < 2; rep++) {  // first pass warms caches and code
-      CK(cudaEventRecord(c->ev[4], c->stream));
+      CK(cudaEventRecord(c->ev[8], c->stream));
       int rc = run_device(c, slice, c->d_rnd, stride, c->d_status, c->d_omc, nullptr, nullptr,
                           c->stream, G, block);
       if (rc) return rc;
-      CK(cudaEventRecord(c->ev[5], c->stream));
-      CK(cudaEventSynchronize(c->ev[5]));
+      CK(cudaEventRecord(c->ev[9], c->stream));
+      CK(cudaEventSynchronize(c->ev[9]));
       float ms = 0;
-      CK(cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]));
+      CK(cudaEventElapsedTime(&ms, c->ev[8], c->ev[9]));
       if (rep == 1 && ms < best) { best = ms; bestG = G; }
     }
   }
@@ -400,8 +497,9 @@ int ccs_create(ccs_ctx **out, int device) {
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(CCS_ERR_CUDA);
   for (auto &e : c->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return bail(CCS_ERR_CUDA);
-  if (cudaMalloc(&c->d_work, 9 * sizeof(unsigned long long)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
+  if (cudaMalloc(&c->d_work, 11 * sizeof(unsigned long long)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
   if (cudaMalloc(&c->d_error, sizeof(int)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
+  if (cudaMalloc(&c->d_kparams, sizeof(KParams)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
   *out = c;
   return CCS_OK;
 }
@@ -412,7 +510,8 @@ void ccs_destroy(ccs_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_target(c);
   dfree(c->d_vtab_v); dfree(c->d_vtab_s);
-  dfree(c->d_work); dfree(c->d_error); dfree(c->d_rnd);
+  dfree(c->d_work); dfree(c->d_error); dfree(c->d_rnd); dfree(c->d_kparams); dfree(c->d_park);
+  dfree(c->d_key); dfree(c->d_key2); dfree(c->d_idx); dfree(c->d_idx2); dfree(c->d_sort_tmp);
   dfree(c->d_status); dfree(c->d_omc); dfree(c->d_steps); dfree(c->d_visits);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -438,8 +537,8 @@ int ccs_set_params(ccs_ctx *c, const ccs_params *p) {
   const int G = p->lanes_per_traj;
   if (G != 0 && G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32)
     return fail(c, CCS_ERR_INVALID, "lanes_per_traj must be 0 or a power of two up to 32");
-  if (p->block_size != 0 && (p->block_size % 32 || p->block_size > MAX_BLOCK || p->block_size < 32))
-    return fail(c, CCS_ERR_INVALID, "block_size must be a multiple of 32 up to %d", MAX_BLOCK);
+  if (p->block_size != 0 && p->block_size != BLOCK)
+    return fail(c, CCS_ERR_INVALID, "block_size must be 0 or %d", BLOCK);
   if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
   const bool vel_changed = !c->have_params || c->p.mu != p->mu || c->p.temperature != p->temperature;
   c->p = *p;
@@ -585,10 +684,10 @@ int ccs_run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int
   if (!d_rnd || !d_status || !d_omc || stride < n) return fail(c, CCS_ERR_INVALID, "bad device buffers");
   if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-  const int block = c->p.block_size ? c->p.block_size : 128;
+  const int block = BLOCK;
   if (!c->tuned_G) {
     // tune on the caller's inputs (outputs land in the context's own buffers)
-    int rc = ensure_run_buffers(c, std::min<size_t>(n, (size_t)c->sm_count * 64), false);
+    int rc = ensure_run_buffers(c, std::min<size_t>(n, (size_t)c->sm_count * 256), false);
     if (rc) return rc;
     if (c->p.lanes_per_traj > 0) c->tuned_G = c->p.lanes_per_traj;
     else {
@@ -633,7 +732,7 @@ int ccs_run(ccs_ctx *c, size_t n, const double *const rnd[9], int8_t *status, do
   for (int k = 0; k < nrows; k++)
     CK(cudaMemcpyAsync(c->d_rnd + (size_t)k * n, rnd[k], n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaEventRecord(c->ev[1], c->stream));
-  const int block = c->p.block_size ? c->p.block_size : 128;
+  const int block = BLOCK;
   rc = autotune(c, n, n, block);
   if (rc) return rc;
   CK(cudaEventRecord(c->ev[2], c->stream));

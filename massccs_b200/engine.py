@@ -32,6 +32,7 @@ class CcsParams(ctypes.Structure):
         ("lanes_per_traj", ctypes.c_int32), ("block_size", ctypes.c_int32),
         ("max_steps_per_try", ctypes.c_uint32),
         ("watchdog_s", ctypes.c_double),
+        ("schedule", ctypes.c_int32), ("park_steps", ctypes.c_uint32),
     ]
 
 
@@ -39,10 +40,11 @@ class CcsStats(ctypes.Structure):
     _fields_ = [
         ("ntraj", ctypes.c_uint64), ("nfree", ctypes.c_uint64), ("nscatter", ctypes.c_uint64),
         ("nlost", ctypes.c_uint64), ("ncapped", ctypes.c_uint64),
-        ("steps", ctypes.c_uint64), ("visits", ctypes.c_uint64), ("force_calls", ctypes.c_uint64),
+        ("steps", ctypes.c_uint64), ("visits", ctypes.c_uint64), ("parked", ctypes.c_uint64),
         ("kernel_ms", ctypes.c_double), ("h2d_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double),
         ("lanes_per_traj", ctypes.c_int32), ("block_size", ctypes.c_int32),
         ("grid_size", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("lane_ms", ctypes.c_double), ("warp_ms", ctypes.c_double),
     ]
 
     def as_dict(self):

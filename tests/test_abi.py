@@ -1,0 +1,57 @@
+"""The C-ABI library builds, loads without a GPU and exports every declared symbol."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared(header):
+    txt = open(os.path.join(ROOT, "include", header)).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(ccs_[a-z_]+|mh_[a-z_]+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from massccs_b200 import build, engine
+    build.build_engine()
+    return engine.load_library()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    from massccs_b200 import engine
+    names = declared("massccs_gpu.h")
+    assert set(names) == set(engine.EXPORTS)
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_abi_version_and_strings(lib):
+    v = ctypes.c_int32(0)
+    assert lib.ccs_version(ctypes.byref(v)) == 0 and v.value == 1
+    assert lib.ccs_status_string(0) == b"ok"
+    assert lib.ccs_status_string(-4) == b"device watchdog expired"
+    assert lib.ccs_last_error(None) == b"no context"
+
+
+def test_params_default_matches_reference_defaults(lib):
+    from massccs_b200 import engine
+    p = engine.default_params()
+    # Constants.h:69-83 defaults
+    assert (p.dt, p.temperature, p.lj_cutoff, p.coul_cutoff, p.skin) == (10.0, 298.0, 12.0, 25.0, 0.01)
+    assert p.gas == 1 and p.force_type == 4 and p.precision == 0
+
+
+def test_create_without_device_fails_cleanly(lib):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a device is present")
+    except ImportError:
+        pass
+    h = ctypes.c_void_p()
+    assert lib.ccs_create(ctypes.byref(h), 0) == -5  # CCS_ERR_NODEVICE
+    assert not h.value

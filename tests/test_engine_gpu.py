@@ -1,0 +1,107 @@
+"""Parity of the CUDA engine with the FP64 oracle, through the C-ABI (GPU).
+
+Bars (stated here, used below):
+  FP64 engine mode: per-pair force sums to 1e-9 relative; setup identical hit
+    flags and positions to 1e-12; per trajectory the same status and
+    1-cos(chi) to 1e-7 on >= 97 % of trajectories (the rest are chaotic
+    orbits, which differ even between two builds of the reference).
+  FP32 engine mode (the production mode): forces to 2e-4 relative (norm-wise,
+    against the oracle's |f| + 1e-3 kcal/mol/A); status agreement >= 97 %;
+    paired CCS within 0.5 % of the oracle's on identical initial conditions.
+"""
+import numpy as np
+import pytest
+
+from helpers import engine_for, oracle_system, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _points(sys_, n, rng, near=True):
+    t = sys_.target()
+    a = rng.integers(0, len(t["x"]), n)
+    base = np.stack([t["x"][a], t["y"][a], t["z"][a]], 1)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = rng.uniform(2.6, 30.0, size=(n, 1)) if near else rng.uniform(20, 60, size=(n, 1))
+    return base + d * r
+
+
+CASES = [("c60.xyz", "He", 4), ("c60.xyz", "He", 2), ("c60.xyz", "He", 1), ("c60.xyz", "Ar", 4),
+         ("04_1ubq_charge_4e_min.pqr", "He", 4), ("04_1ubq_charge_4e_min.pqr", "N2", 6),
+         ("04_1ubq_charge_4e_min.pqr", "N2", 4), ("04_1ubq_charge_4e_min.pqr", "N2", 3),
+         ("04_1ubq_charge_4e_min.pqr", "CO2", 6), ("c60.xyz", "CO2", 4), ("c60.xyz", "co2", 2)]
+
+
+@pytest.mark.parametrize("target,gas,ft", CASES)
+@pytest.mark.parametrize("prec", [1, 0])
+def test_site_forces_match_oracle(oracle, target, gas, ft, prec):
+    s = oracle_system(oracle, target=target, gas=gas, ft=ft)
+    eng = engine_for(s, precision=prec)
+    rng = np.random.default_rng(7)
+    pts = np.concatenate([_points(s, 300, rng), _points(s, 50, rng, near=False)])
+    nsite = 3 if gas in ("N2", "CO2") else 1
+    for site in range(nsite):
+        f, U, _ = eng.eval_site_forces(site, pts)
+        fo = np.empty_like(f)
+        Uo = np.empty_like(U)
+        for i, p in enumerate(pts):
+            fo[i], Uo[i], _ = s.site_force(site, p)
+        tol = 1e-9 if prec == 1 else 2e-4
+        scale = np.linalg.norm(fo, axis=1) + 1e-3
+        err = np.linalg.norm(f - fo, axis=1) / scale
+        assert err.max() < tol, (site, err.max())
+        uerr = np.abs(U - Uo) / (np.abs(Uo) + 1e-3)
+        assert uerr.max() < tol, (site, uerr.max())
+
+
+@pytest.mark.parametrize("gas", ["He", "N2", "CO2"])
+def test_setup_matches_oracle(oracle, gas):
+    s = oracle_system(oracle, gas=gas, ft=4)
+    eng = engine_for(s, precision=1)
+    rnd = s.predraw(4000)
+    hit, pos, vel = eng.eval_setup(rnd)
+    ns = 3 if gas in ("N2", "CO2") else 1
+    for j in range(0, 4000, 7):
+        h, p, v, _, _ = s.setup_one(rnd[:, j])
+        assert h == hit[j]
+        if h:
+            np.testing.assert_allclose(pos[j, :ns], p[:ns], rtol=1e-12, atol=1e-10)
+            np.testing.assert_allclose(vel[j, :ns], v[:ns], rtol=1e-11, atol=1e-15)
+
+
+def _paired(oracle, target, gas, ft, n, prec, quirks=0, **kw):
+    s = oracle_system(oracle, target=target, gas=gas, ft=ft, nprobe=n)
+    rnd = s.predraw(n)
+    ref = s.run(rnd, quirks=quirks)
+    eng = engine_for(s, precision=prec, quirks=quirks, **kw)
+    out = eng.run(rnd)
+    return s, ref, out
+
+
+TRAJ = [("c60.xyz", "He", 4, 3000), ("c60.xyz", "Ar", 4, 2000),
+        ("04_1ubq_charge_4e_min.pqr", "He", 4, 1500), ("c60.xyz", "N2", 6, 1000),
+        ("04_1ubq_charge_4e_min.pqr", "N2", 6, 600), ("c60.xyz", "CO2", 4, 800)]
+
+
+@pytest.mark.parametrize("target,gas,ft,n", TRAJ)
+def test_trajectories_fp64_match_oracle(oracle, target, gas, ft, n):
+    s, ref, out = _paired(oracle, target, gas, ft, n, prec=1)
+    same = out["status"] == ref["status"]
+    assert same.mean() >= 0.97
+    close = same & (np.abs(out["one_minus_cos"] - ref["one_minus_cos"]) <= 1e-7)
+    assert close.mean() >= 0.97, close.mean()
+    st = out["stats"]
+    assert st["nfree"] + st["nscatter"] + st["nlost"] + st["ncapped"] == n
+
+
+@pytest.mark.parametrize("target,gas,ft,n", TRAJ)
+@pytest.mark.parametrize("lanes", [0, 1, 32])
+def test_trajectories_fp32_paired_ccs(oracle, target, gas, ft, n, lanes):
+    s, ref, out = _paired(oracle, target, gas, ft, n, prec=0, lanes_per_traj=lanes)
+    P = s.params
+    assert (out["status"] == ref["status"]).mean() >= 0.97
+    bmax = P["bmax"]
+    w_ref = np.pi * ref["one_minus_cos"][ref["status"] == 1].sum() * bmax ** 2 / ((ref["status"] <= 1).sum())
+    w_gpu = np.pi * out["one_minus_cos"][out["status"] == 1].sum() * bmax ** 2 / ((out["status"] <= 1).sum())
+    assert rel(w_gpu, w_ref) <= 0.005, (w_gpu, w_ref)
