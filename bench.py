@@ -1,0 +1,358 @@
+"""Benchmark of the trajectory-method CCS hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config globule_n2|c60_he]
+    python bench.py --impl reference ...   # the reference's own CPU implementation
+
+One step = one pass of the trajectory loop over the workload's trajectories:
+the charged 1231-atom globule with the 3-site N2 probe, 3e5 trajectories (the
+configuration the headline metric is quoted on; `--config c60_he` runs the
+60-atom cage with He).  Prints one JSON line.
+
+value      trajectories/s with the random inputs resident in HBM (ccs_run_device),
+           whole job over all ranks (each rank its own trajectories: weak scaling)
+e2e        the same metric through the public host API (mh_predraw on the host,
+           ccs_run with pinned host buffers: H2D of the inputs and D2H of the
+           per-trajectory results inside the timed region, then the reduction)
+roofline   FP32-pipe roofline of the trajectory kernels: algorithmic flops (the
+           reference's target-atom visits per trajectory x flops per visit) over
+           the device time, against the device's measured FP32 FMA peak
+cpu_baseline  the reference binary (oracle/_ref/massccs) on this host's cores,
+           on a bounded sample of the same workload
+"""
+import argparse
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "trajectories/s on 1 B200 at <=0.5% CCS err vs FP64: plain FP32 vs surrogate vs CPU"
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "massccs")
+
+# flops per target-atom visit of one probe site (fixed constants of the work
+# model): LJ + induced dipole 45, LJ + Coulomb 25, Coulomb + induced dipole 40,
+# LJ only 20
+FLOPS_PER_VISIT = {("He", 4): 45.0, ("N2", 6): (25.0 + 25.0 + 40.0) / 3.0}
+
+CONFIGS = {
+    "globule_n2": dict(gen="globule_n2", ntraj=300000, nprobe=30000, niter=10, gas="N2", ft=6,
+                       desc="1231-atom globule (Rg 11.5 A, +4 e), N2 3-site, force type 6, 3e5 trajectories"),
+    "c60_he": dict(gen="c60_he", ntraj=300000, nprobe=30000, niter=10, gas="He", ft=4,
+                   desc="60-atom C60 cage (C-C 1.40 A, neutral, uff.ff), He, force type 4, 3e5 trajectories"),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_workload(name, d):
+    from massccs_b200 import synth
+    c = CONFIGS[name]
+    gen = getattr(synth, c["gen"])
+    return gen(d, nprobe=c["nprobe"], niter=c["niter"])
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle samples while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi") is None:
+            return self
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def ref_sample_run(json_path, nprobe, niter, threads):
+    """Run the reference binary on a sample; returns (trajectories, CCS time s, ccs)."""
+    d = os.path.dirname(json_path)
+    cfg = json.load(open(json_path))
+    cfg.update({"numberProbe": nprobe, "nIter": niter, "nthreads": threads})
+    p = os.path.join(d, "input_ref.json")
+    json.dump(cfg, open(p, "w"))
+    out = subprocess.run([REF_BIN, "input_ref.json"], cwd=d, capture_output=True, text=True, timeout=1800)
+    m = re.search(r"CCS time: (\S+) s", out.stdout)
+    c = re.search(r"average value of CCS = (\S+)", out.stdout)
+    if out.returncode != 0 or not m:
+        raise RuntimeError("reference run failed: " + out.stderr[-400:])
+    return nprobe * niter, float(m.group(1)), float(c.group(1)) if c else None
+
+
+def cpu_baseline(json_path, config):
+    """The reference binary on this host's cores, on a bounded sample, plus the
+    reference's visit count per trajectory (from the oracle, on a smaller
+    sample) for the roofline's algorithmic work."""
+    threads = os.cpu_count() or 1
+    out = {"value": None, "unit": "trajectories/s", "cores": threads, "kind": "reference", "sample": None}
+    visits = None
+    if os.path.exists(REF_BIN):
+        # about 10-30 s of CPU work: probe with a small run, then size the sample
+        n0, t0, _ = ref_sample_run(json_path, 200, 5, threads)
+        rate = n0 / max(t0, 1e-3)
+        target = int(min(max(rate * 15.0, 2000), 200000))
+        niter = 10
+        nprobe = max(100, target // niter)
+        n, t, _ = ref_sample_run(json_path, nprobe, niter, threads)
+        out.update(value=n / t, sample=f"{n} trajectories ({nprobe} x {niter}) of the {config} workload, "
+                                           f"seed of the workload, nthreads {threads}; CCS time {t:.2f} s")
+    try:
+        from oracle import pyoracle
+        sys_ = pyoracle.OracleSystem(json_path)
+        m = 400
+        res = sys_.run(sys_.predraw(m), nthreads=threads)
+        visits = float(res["visits"].mean())
+    except Exception as e:  # the roofline then reports the engine's own count only
+        log("oracle visit count unavailable:", e)
+    return out, visits
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    cfg = CONFIGS[args.config]
+    line = {"metric": METRIC, "impl": "reference", "unit": "trajectories/s", "higher_is_better": True,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": args.config, "description": cfg["desc"]}}
+    if not os.path.exists(REF_BIN):
+        line["unavailable"] = "reference binary oracle/_ref/massccs not built (make -C oracle ref)"
+        print(json.dumps(line), flush=True)
+        return
+    d = tempfile.mkdtemp(prefix="bench_ref_")
+    json_path = make_workload(args.config, d)
+    threads = os.cpu_count() or 1
+    n0, t0, _ = ref_sample_run(json_path, 200, 5, threads)
+    rate = n0 / max(t0, 1e-3)
+    per_step = int(min(max(rate * 8.0, 2000), 200000))  # ~8 s of CPU work per step
+    nprobe, niter = max(100, per_step // 10), 10
+    for _ in range(args.warmup):
+        ref_sample_run(json_path, max(100, nprobe // 10), niter, threads)
+    times, n = [], 0
+    for _ in range(args.steps):
+        k, t, _ = ref_sample_run(json_path, nprobe, niter, threads)
+        times.append(t)
+        n = k
+    total = sum(times)
+    value = n * len(times) / total
+    line.update(value=value, ms_per_step=1e3 * total / len(times),
+                cpu_baseline={"value": value, "unit": "trajectories/s", "cores": threads, "kind": "reference",
+                              "sample": f"{n} trajectories per step ({nprobe} x {niter}), nthreads {threads}"},
+                e2e={"value": value, "unit": "trajectories/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    shutil.rmtree(d, ignore_errors=True)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="globule_n2", choices=sorted(CONFIGS))
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":  # CPU only: rank 0 runs it, the other ranks have nothing to do
+        run_reference_arm(args, rank, world)
+        return
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        import torch
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist = dist_mod
+
+    import numpy as np
+    import torch
+    from massccs_b200 import engine as E
+    from massccs_b200 import host as H
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    cfg = CONFIGS[args.config]
+    d = tempfile.mkdtemp(prefix=f"bench_{rank}_")
+    json_path = make_workload(args.config, d)
+    S = H.System(json_path)
+    n = cfg["ntraj"]
+    seed = S.info["seed"] + rank  # each rank its own trajectories
+    rnd_host = S.predraw(n, seed=seed)
+    eng = S.engine(device=local)
+    stream = torch.cuda.current_stream(dev)
+    d_rnd = torch.from_numpy(rnd_host).to(dev)
+    d_status = torch.empty(n, dtype=torch.int8, device=dev)
+    d_omc = torch.empty(n, dtype=torch.float64, device=dev)
+    d_steps = torch.empty(n, dtype=torch.int32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
+
+    def step_device():
+        eng.run_device(n, d_rnd.data_ptr(), n, d_status.data_ptr(), d_omc.data_ptr(), d_steps.data_ptr(), 0,
+                       stream.cuda_stream)
+
+    log(f"[rank {rank}] warmup x{args.warmup} on {cfg['desc']}")
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+    stats = eng.sync_stats()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            step_device()
+            ev[k][1].record(stream)
+        barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    last = eng.sync_stats()
+    dev_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([dev_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    ms_per_step = dev_ms / args.steps
+    value = world * n / (ms_per_step * 1e-3)
+
+    # e2e through the public API: pre-draw on the host into pinned memory,
+    # ccs_run (H2D, both passes, D2H), the reduction; every step
+    pin = torch.empty((9, n), dtype=torch.float64).pin_memory()
+    pin_np = pin.numpy()
+    st_pin = torch.empty(n, dtype=torch.int8).pin_memory().numpy()
+    om_pin = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    rows = (__import__("ctypes").c_void_p * 9)(*[pin_np[k].ctypes.data for k in range(9)])
+    import ctypes
+    L = E.load_library()
+    HL = H.load_library()
+
+    def step_e2e():
+        HL.mh_predraw(S._h, seed, n, pin_np.ctypes.data_as(ctypes.c_void_p))
+        stt = E.CcsStats()
+        rc = L.ccs_run(eng._h, n, rows, st_pin.ctypes.data_as(ctypes.c_void_p),
+                       om_pin.ctypes.data_as(ctypes.c_void_p), None, None, ctypes.byref(stt))
+        if rc:
+            raise E.CcsError(L.ccs_last_error(eng._h).decode())
+        H.reduce(S.info["niter"], S.info["nprobe"], st_pin, om_pin, S.info["bmax"])
+
+    step_e2e()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_e2e()
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if dist:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * n / e2e_s
+
+    if rank == 0:
+        status = st_pin
+        nscatter = int((status == 1).sum())
+        peak = E.measure_fp32_peak(local)
+        engine_visits = last["visits"] / max(1, n)
+        ref_visits = None
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu, ref_visits = cpu_baseline(json_path, args.config)
+        fpv = FLOPS_PER_VISIT.get((cfg["gas"], cfg["ft"]), 30.0)
+        kernel_s = ms_per_step * 1e-3
+        alg_visits = ref_visits if ref_visits else engine_visits
+        achieved = n * alg_visits * fpv / kernel_s / 1e12
+        traffic = None
+        prof = os.path.join(ROOT, "profiles", f"traffic_{args.config}.json")
+        if os.path.exists(prof):
+            traffic = json.load(open(prof)).get("bytes_per_launch")
+        line = {
+            "metric": METRIC, "value": value, "unit": "trajectories/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.config, "description": cfg["desc"], "trajectories_per_gpu": n,
+                       "l2": "256 MiB buffer written between timed steps (outside the step events)",
+                       "parallelism": f"{world} ranks, independent trajectory shards"},
+            "e2e": {"value": e2e_value, "unit": "trajectories/s", "h2d_bytes_per_step": 9 * 8 * n,
+                    "d2h_bytes_per_step": 9 * n,
+                    "includes": "host mt19937 pre-draw, H2D, lane+warp passes, D2H, reduction"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if peak else None, "traffic": traffic,
+                         "peak_source": "FP32 FMA-chain kernel (ccs_measure_fp32_peak) on this device",
+                         "work": ("reference target-atom visits per trajectory (oracle, reference cells) "
+                                  if ref_visits else "engine candidate visits per trajectory ") +
+                                 f"{alg_visits:.4g} x {fpv:g} flops per visit",
+                         "engine_visits_per_traj": engine_visits,
+                         "engine_tflops": n * engine_visits * fpv / kernel_s / 1e12},
+            "cpu_baseline": cpu,
+            "gpu_launches": 3 * args.steps,
+            "engine": {"lane_ms": last["lane_ms"], "warp_ms": last["warp_ms"], "parked": last["parked"],
+                       "lanes_per_force": last["lanes_per_traj"], "scatter_fraction": nscatter / n,
+                       "steps_per_traj": last["steps"] / n},
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    shutil.rmtree(d, ignore_errors=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

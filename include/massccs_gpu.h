@@ -174,6 +174,12 @@ typedef struct {
 } ccs_info;
 int ccs_get_info(ccs_ctx *ctx, ccs_info *info);
 
+/* Measurement helper with no counterpart in the reference: the device's
+ * sustained FP32 FMA throughput (TFLOP/s, 2 flops per FMA), measured by an
+ * FMA-chain kernel over all SMs for about `ms` milliseconds.  The trajectory
+ * kernels are bound by the FP32 pipe, so this is their roofline denominator. */
+int ccs_measure_fp32_peak(int device, double ms, double *tflops);
+
 /* Human-readable strings. */
 const char *ccs_status_string(int status);
 const char *ccs_last_error(ccs_ctx *ctx);

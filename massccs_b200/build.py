@@ -76,16 +76,16 @@ def build_host(force=False):
     lib_out = os.path.join(LIB, "libmassccs_host.so")
     deps = cpp + hdr + [os.path.join(INC, f) for f in os.listdir(INC)]
     gxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
-    cuda_lib = "/usr/local/cuda/lib64"
-    if force or _newer(lib_out, deps):
-        _run([gxx] + HOST_FLAGS + ["-shared", "-I", INC, "-o", lib_out] + cpp)
+    engine = os.path.join(LIB, "libmassccs_gpu.so")
+    if force or _newer(lib_out, deps + [engine]):
+        _run([gxx] + HOST_FLAGS + ["-shared", "-I", INC, "-o", lib_out] + cpp +
+             ["-L", LIB, "-lmassccs_gpu", "-Wl,-rpath,$ORIGIN"])
     main = os.path.join(hdir, "main.cpp")
     exe = os.path.join(BIN, "massccs")
     if os.path.exists(main) and (force or _newer(exe, deps + [main, lib_out])):
         _run([gxx] + HOST_FLAGS + ["-I", INC, "-o", exe, main,
                                    "-L", LIB, "-lmassccs_host", "-lmassccs_gpu",
-                                   "-Wl,-rpath,$ORIGIN/../lib", "-L", cuda_lib, "-lcudart",
-                                   "-Wl,-rpath," + cuda_lib])
+                                   "-Wl,-rpath,$ORIGIN/../lib"])
     return lib_out
 
 

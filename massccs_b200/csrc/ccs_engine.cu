@@ -828,6 +828,57 @@ int ccs_eval_setup(ccs_ctx *c, size_t n, const double *const rnd[9], int8_t *hit
   return CCS_OK;
 }
 
+}  // extern "C"
+
+// FP32 FMA throughput kernel: 8 independent chains per thread, each step one FMA.
+__global__ void fma_peak_kernel(float *out, int iters, float a, float b) {
+  float x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6,
+        x7 = x0 + 7;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+      x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+      x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+    }
+  }
+  const float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == 123.456f) out[blockIdx.x] = s;  // keeps the chains live
+}
+
+extern "C" {
+
+int ccs_measure_fp32_peak(int device, double ms, double *tflops) {
+  if (!tflops) return CCS_ERR_INVALID;
+  ccs_ctx *c = nullptr;  // CK() reports into no context here
+  if (cudaSetDevice(device) != cudaSuccess) return CCS_ERR_NODEVICE;
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  float *out = nullptr;
+  CK(cudaMalloc(&out, 4096 * sizeof(float)));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int threads = 256, blocks = prop.multiProcessorCount * 8;
+  int iters = 256;
+  float best = 0;
+  for (int rep = 0; rep < 6; rep++) {
+    CK(cudaEventRecord(e0));
+    fma_peak_kernel<<<blocks, threads>>>(out, iters, 0.999999f, 1e-7f);
+    CK(cudaEventRecord(e1));
+    CK(cudaEventSynchronize(e1));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
+    best = std::max(best, (float)(flops / (t * 1e-3) / 1e12));
+    if (t < ms && rep < 5) iters = (int)std::min<double>(1 << 22, iters * std::max(1.0, ms / std::max(t, 0.01f)));
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  *tflops = best;
+  return CCS_OK;
+}
+
 const char *ccs_status_string(int s) {
   switch (s) {
     case CCS_OK: return "ok";

@@ -72,7 +72,8 @@ class CcsInfo(ctypes.Structure):
 # Every symbol include/massccs_gpu.h declares.
 EXPORTS = ["ccs_version", "ccs_create", "ccs_destroy", "ccs_params_default", "ccs_set_target",
            "ccs_set_params", "ccs_run", "ccs_run_device", "ccs_sync_stats", "ccs_eval_site_forces",
-           "ccs_eval_setup", "ccs_get_info", "ccs_status_string", "ccs_last_error"]
+           "ccs_eval_setup", "ccs_get_info", "ccs_status_string", "ccs_last_error",
+           "ccs_measure_fp32_peak"]
 
 _LIB = None
 
@@ -105,6 +106,7 @@ def load_library(path=LIB_PATH):
     L.ccs_status_string.restype = ctypes.c_char_p
     L.ccs_last_error.argtypes = [vp]
     L.ccs_last_error.restype = ctypes.c_char_p
+    L.ccs_measure_fp32_peak.argtypes = [i32, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
     if path == LIB_PATH:
         _LIB = L
     return L
@@ -228,6 +230,15 @@ class Engine:
         self._check(self._L.ccs_eval_setup(self._h, n, ptrs, _p(hit), _p(pos), _p(vel)),
                     "ccs_eval_setup")
         return hit, pos, vel
+
+
+def measure_fp32_peak(device=0, ms=200.0):
+    """Sustained FP32 FMA TFLOP/s of the device (the plain path's roofline)."""
+    v = ctypes.c_double(0)
+    rc = load_library().ccs_measure_fp32_peak(device, ms, ctypes.byref(v))
+    if rc != 0:
+        raise CcsError(f"ccs_measure_fp32_peak failed: {rc}")
+    return v.value
 
 
 def params_from_system(sp, precision=PREC_FP32, quirks=0, **kw):

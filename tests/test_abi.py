@@ -11,22 +11,31 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def declared(header):
     txt = open(os.path.join(ROOT, "include", header)).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(ccs_[a-z_]+|mh_[a-z_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(ccs_[a-z0-9_]+|mh_[a-z0-9_]+)\s*\(", txt)))
 
 
 @pytest.fixture(scope="module")
 def lib():
     from massccs_b200 import build, engine
-    build.build_engine()
+    build.build()
     return engine.load_library()
 
 
 def test_every_declared_symbol_is_exported(lib):
-    from massccs_b200 import engine
+    from massccs_b200 import engine, host
     names = declared("massccs_gpu.h")
     assert set(names) == set(engine.EXPORTS)
     for n in names:
         assert hasattr(lib, n), n
+    hl = host.load_library()
+    hnames = declared("massccs_host.h")
+    assert set(hnames) == set(host.EXPORTS)
+    for n in hnames:
+        assert hasattr(hl, n), n
+
+
+def test_cli_is_built():
+    assert os.access(os.path.join(ROOT, "massccs_b200", "bin", "massccs"), os.X_OK)
 
 
 def test_abi_version_and_strings(lib):

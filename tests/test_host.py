@@ -1,0 +1,101 @@
+"""The product's host set-up (libmassccs_host.so) against the oracle (CPU).
+
+The host re-implements the reference's Input / GasBuffer / MoleculeTarget /
+ellipsoid / pre-draw / reduction in C++; every one of them must reproduce the
+oracle's restatement exactly (bit-exact scalars and arrays), because the GPU
+engine's parity is only meaningful on identical inputs.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN, input_dict, workdir, write_input
+
+CASES = [("c60.xyz", "He", 4, None), ("c60.xyz", "Ar", 4, None), ("c60.xyz", "N2", 6, None),
+         ("c60.xyz", "CO2", 6, None), ("c60.xyz", "co2", 2, None), ("c60.xyz", "He", 1, None),
+         ("04_1ubq_charge_4e_min.pqr", "He", 4, None), ("04_1ubq_charge_4e_min.pqr", "N2", 4, None),
+         ("c60.xyz", "He", 2, "uff.ff"), ("04_1ubq_charge_4e_min.pqr", "CO2", 4, "uff.ff")]
+
+
+@pytest.fixture(scope="module")
+def host():
+    from massccs_b200 import build, host
+    build.build()
+    return host
+
+
+def _sorted_target(t):
+    keys = ("x", "y", "z", "q", "m", "eps", "sig")
+    arr = np.stack([t[k] for k in keys], 1)
+    return arr[np.lexsort(arr[:, :3].T[::-1])]
+
+
+@pytest.mark.parametrize("target,gas,ft,ff", CASES)
+def test_setup_matches_oracle(oracle, host, target, gas, ft, ff):
+    d = workdir()
+    p = write_input(d, input_dict(target, gas, ft, nprobe=50, niter=2, ff=ff))
+    S = host.System(p)
+    O = oracle.OracleSystem(p)
+    hi, oi = S.info, O.params
+    for k in ("gas_flag", "force_type", "natoms", "gas_natoms", "nprobe", "niter", "seed", "Nx", "Ny", "Nz"):
+        assert hi[k] == oi[k], k
+    for k in ("dt", "temperature", "skin", "lj_cutoff", "coul_cutoff", "alpha", "mu", "target_mass",
+              "target_charge", "gas_mass", "gas_inertia", "d_bond", "a", "b", "c", "bmax", "lx", "ly", "lz",
+              "max_x", "max_y", "max_z", "radius"):
+        assert hi[k] == oi[k], (k, hi[k], oi[k])
+    # the oracle keeps the reference's cell order; compare as sorted sets, bit-exact
+    np.testing.assert_array_equal(_sorted_target(S.target()), _sorted_target(O.target()))
+    if gas == "CO2":
+        ts, to = S.target(), O.target()
+        np.testing.assert_array_equal(np.sort(ts["eps_c"]), np.sort(to["eps_c"]))
+        np.testing.assert_array_equal(np.sort(ts["sig_c"]), np.sort(to["sig_c"]))
+
+
+@pytest.mark.parametrize("gas", ["He", "N2"])
+def test_predraw_matches_oracle(oracle, host, gas):
+    d = workdir()
+    p = write_input(d, input_dict("c60.xyz", gas, 4, nprobe=300, niter=3))
+    S, O = host.System(p), oracle.OracleSystem(p)
+    np.testing.assert_array_equal(S.predraw(), O.predraw(900))
+
+
+def test_reduction_matches_oracle(oracle, host):
+    rng = np.random.default_rng(0)
+    status = rng.choice([0, 1, 1, 1, 2], size=5000).astype(np.int8)
+    omc = np.where(status == 1, rng.random(5000) * 2, 0.0)
+    a = host.reduce(10, 500, status, omc, 53.6)
+    b = oracle.reduce(10, 500, status, omc, 53.6)
+    np.testing.assert_array_equal(a["omega"], b["omega"])
+    np.testing.assert_array_equal(a["nfree"], b["nfree"])
+    assert a["ccs"] == b["ccs"] and a["err"] == b["err"]
+
+
+def test_input_errors_are_reported(host):
+    d = workdir()
+    p = os.path.join(d, "bad.json")
+    json.dump({"numberProbe": 10}, open(p, "w"))
+    with pytest.raises(Exception, match="targetFileName"):
+        host.System(p)
+    p2 = write_input(d, dict(input_dict("c60.xyz"), GasBuffer="Xe"), name="bad2.json")
+    with pytest.raises(Exception, match="gas buffer"):
+        host.System(p2)
+    p3 = write_input(d, input_dict("missing.xyz"), name="bad3.json")
+    with pytest.raises(Exception):
+        host.System(p3)
+
+
+def test_synthetic_targets(host):
+    from massccs_b200 import synth
+    d = workdir(())
+    S = host.System(synth.c60_he(os.path.join(d, "c60"), nprobe=10, niter=1))
+    t = S.target()
+    xyz = np.stack([t["x"], t["y"], t["z"]], 1)
+    dist = np.linalg.norm(xyz[:, None] - xyz[None], axis=2)
+    np.fill_diagonal(dist, 9)
+    assert S.info["natoms"] == 60 and abs(dist.min() - 1.40) < 1e-6
+    assert ((np.abs(dist - 1.40) < 1e-6).sum() // 2) == 90  # the 90 edges of a truncated icosahedron
+    G = host.System(synth.globule_n2(os.path.join(d, "glob"), nprobe=10, niter=1))
+    assert G.info["natoms"] == 1231 and abs(G.info["target_charge"] - 4.0) < 1e-5
+    assert G.info["force_type"] == 6 and G.info["gas_flag"] == 2
