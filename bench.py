@@ -230,7 +230,8 @@ def main():
     seed = S.info["seed"] + rank  # each rank its own trajectories
     rnd_host = S.predraw(n, seed=seed)
     eng = S.engine(device=local)
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)  # a real stream handle (0 would mean the engine's own stream)
+    torch.cuda.set_stream(stream)
     d_rnd = torch.from_numpy(rnd_host).to(dev)
     d_status = torch.empty(n, dtype=torch.int8, device=dev)
     d_omc = torch.empty(n, dtype=torch.float64, device=dev)
@@ -253,6 +254,7 @@ def main():
         torch.cuda.synchronize()
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    per_step = []
     barrier()
     with ClockSampler(local) as clocks:
         for k in range(args.steps):
@@ -260,9 +262,12 @@ def main():
             ev[k][0].record(stream)
             step_device()
             ev[k][1].record(stream)
+            per_step.append(eng.sync_stats())  # host sync after the step's stop event
         barrier()
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    last = eng.sync_stats()
+    last = per_step[-1]
+    log(f"[rank {rank}] steps (ms): " + ", ".join(f"{t:.1f} (lane {st['lane_ms']:.1f}, warp {st['warp_ms']:.1f},"
+                                                  f" parked {st['parked']})" for t, st in zip(step_ms, per_step)))
     dev_ms = sum(step_ms)
     if dist:
         t = torch.tensor([dev_ms], device=dev)
@@ -298,6 +303,9 @@ def main():
         step_e2e()
     barrier()
     e2e_s = (time.perf_counter() - t0) / args.steps
+    e2e_stats = eng.sync_stats()
+    log(f"[rank {rank}] e2e step {e2e_s * 1e3:.1f} ms (kernel {e2e_stats['kernel_ms']:.1f}, lane {e2e_stats['lane_ms']:.1f},"
+        f" warp {e2e_stats['warp_ms']:.1f}, h2d {e2e_stats['h2d_ms']:.2f}, d2h {e2e_stats['d2h_ms']:.2f})")
     if dist:
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

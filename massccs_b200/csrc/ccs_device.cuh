@@ -251,7 +251,17 @@ __device__ __forceinline__ void eval_forces(const KParams &kp, const T (&p)[GasS
     const T ex = fmax(fmax(T(kp.bb_lo[0]) - cx, cx - T(kp.bb_hi[0])), T(0));
     const T ey = fmax(fmax(T(kp.bb_lo[1]) - cy, cy - T(kp.bb_hi[1])), T(0));
     const T ez = fmax(fmax(T(kp.bb_lo[2]) - cz, cz - T(kp.bb_hi[2])), T(0));
-    if (ex * ex + ey * ey + ez * ez <= R * R) {
+    // the whole target inside the reach sphere: every atom is a candidate
+    const T fx = fmax(cx - T(kp.bb_lo[0]), T(kp.bb_hi[0]) - cx);
+    const T fy = fmax(cy - T(kp.bb_lo[1]), T(kp.bb_hi[1]) - cy);
+    const T fz = fmax(cz - T(kp.bb_lo[2]), T(kp.bb_hi[2]) - cz);
+    if (fx * fx + fy * fy + fz * fz <= R * R) {
+      for (int ai = g; ai < kp.natoms; ai += G) {
+        const Atom<T> a = load_atom<T, GAS>(kp, ai);
+        visit_atom<T, GAS, HASQ>(kp, p, act, a, acc);
+      }
+      if (G == 1 || g == 0) nvis += (uint32_t)kp.natoms;
+    } else if (ex * ex + ey * ey + ez * ez <= R * R) {
       const T ih = T(kp.inv_h), h = T(kp.h), ox = T(kp.ox), oy = T(kp.oy), oz = T(kp.oz);
       const int i0 = (int)fmax(T(0), floor((cx - R - ox) * ih));
       const int i1 = (int)fmin(T(kp.nx - 1), floor((cx + R - ox) * ih));
@@ -374,7 +384,24 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
     const T ex = fmax(fmax(T(kp.bb_lo[0]) - cx, cx - T(kp.bb_hi[0])), T(0));
     const T ey = fmax(fmax(T(kp.bb_lo[1]) - cy, cy - T(kp.bb_hi[1])), T(0));
     const T ez = fmax(fmax(T(kp.bb_lo[2]) - cz, cz - T(kp.bb_hi[2])), T(0));
-    if (ex * ex + ey * ey + ez * ez <= R * R) {
+    const T fx = fmax(cx - T(kp.bb_lo[0]), T(kp.bb_hi[0]) - cx);
+    const T fy = fmax(cy - T(kp.bb_lo[1]), T(kp.bb_hi[1]) - cy);
+    const T fz = fmax(cz - T(kp.bb_lo[2]), T(kp.bb_hi[2]) - cz);
+    if (fx * fx + fy * fy + fz * fz <= R * R) {
+      // the whole target inside the reach sphere: every atom is a candidate
+      int t = tid;
+      for (; t + NT < kp.natoms; t += 2 * NT) {
+        const Atom<T> a1 = load_atom<T, GAS>(kp, t);
+        const Atom<T> a2 = load_atom<T, GAS>(kp, t + NT);
+        visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
+        visit_atom<T, GAS, HASQ>(kp, p, act, a2, acc);
+      }
+      if (t < kp.natoms) {
+        const Atom<T> a1 = load_atom<T, GAS>(kp, t);
+        visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
+      }
+      nvis += (uint32_t)kp.natoms;
+    } else if (ex * ex + ey * ey + ez * ez <= R * R) {
       const T ih = T(kp.inv_h), h = T(kp.h), ox = T(kp.ox), oy = T(kp.oy), oz = T(kp.oz);
       const int i0 = (int)fmax(T(0), floor((cx - R - ox) * ih));
       const int i1 = (int)fmin(T(kp.nx - 1), floor((cx + R - ox) * ih));
