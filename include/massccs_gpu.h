@@ -152,6 +152,28 @@ int ccs_run_device(ccs_ctx *ctx, size_t ntraj, const double *d_rnd, size_t strid
                    uint32_t *d_visits, void *stream);
 int ccs_sync_stats(ccs_ctx *ctx, ccs_stats *stats);
 
+/* ccs_run_device without any device allocation.  No counterpart in the
+ * reference (whose CPU loop allocates per trajectory): it is for callers that
+ * cannot allocate device memory while they run -- a host whose allocator owns
+ * the whole device heap, a service with a memory budget fixed at start-up, or
+ * code where an allocation would synchronise the device.  The run's scratch
+ * (work counter, statistics, launch-parameter copy, park buffer of long
+ * trajectories) is a 24 MiB static device array that every GPU loading the
+ * library holds until exit; inputs and outputs are the caller's device
+ * buffers, as for ccs_run_device, and the results are the same.
+ *  - at most 262144 trajectories per call (CCS_ERR_INVALID beyond that);
+ *  - the first call on a device looks up the array's device address; make it
+ *    before any stream capture;
+ *  - the array is shared by every call on a device and keeps the last call's
+ *    contents: calls whose work overlaps on the GPU (other streams, other
+ *    threads, other contexts on the same device) race, so serialise them;
+ *  - lanes per force evaluation: the configured value, else the one the
+ *    context already tuned, else 32 (no autotuning run);
+ *  - stats may be NULL; when given, the call waits for the run and fills it. */
+int ccs_run_device_noalloc(ccs_ctx *ctx, size_t ntraj, const double *d_rnd, size_t stride,
+                           int8_t *d_status, double *d_one_minus_cos, uint32_t *d_steps,
+                           uint32_t *d_visits, void *stream, ccs_stats *stats);
+
 /* Force on gas site `site` at npts positions (pos: npts x 3), as the
  * reference's per-site dispatch picks the routine (System.cpp:371-379,
  * 594-637, 1028-1065 -> Force.cpp).  Same device code as the trajectory

@@ -15,6 +15,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -895,3 +896,138 @@ const char *ccs_status_string(int s) {
 const char *ccs_last_error(ccs_ctx *c) { return c ? c->err.c_str() : "no context"; }
 
 }  // extern "C"
+
+// ===========================================================================
+// ccs_run_device_noalloc: the trajectory passes with no device allocation.
+//
+// Some callers cannot allocate device memory while they run: a host that has
+// handed the whole device heap to its own pool allocator, a real-time or
+// embedded service whose memory budget is fixed at start-up, or code running
+// where a cudaMalloc would synchronise the device or fail.  For them the
+// scratch of the trajectory passes (work counter, statistics, the device copy
+// of the launch parameters and the park buffer of long trajectories) lives in
+// this file-scope array instead of per-context allocations.  Every GPU that
+// loads the library holds it until the process exits.
+namespace {
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(24) << 20;  // 24 MiB per device
+constexpr size_t NOALLOC_HEADER_BYTES = 256;                // counters and the error flag
+constexpr size_t NOALLOC_PARAMS_BYTES = 4096;               // the launch-parameter copy
+constexpr size_t NOALLOC_MAX_TRAJ = size_t(1) << 18;        // 262144 trajectories per call
+constexpr size_t NOALLOC_PARK_CAP = 65536;                  // the park capacity ccs_run_device uses for them
+static_assert(sizeof(KParams) <= NOALLOC_PARAMS_BYTES, "launch parameters do not fit");
+static_assert(NOALLOC_HEADER_BYTES + NOALLOC_PARAMS_BYTES + NOALLOC_PARK_CAP * sizeof(LaneState<double>) <=
+                  NOALLOC_SCRATCH_BYTES,
+              "park buffer does not fit");
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// The device-side copy of the launch parameters, written by a kernel so that
+// no host staging is involved.
+__global__ void copy_params_kernel(KParams k, KParams *dst) { *dst = k; }
+
+namespace {
+// device address of g_noalloc_scratch, looked up once per device (with that
+// device current); host code may not use the symbol itself as an address
+struct NoallocSlot {
+  std::once_flag once;
+  unsigned char *ptr = nullptr;
+  cudaError_t err = cudaSuccess;
+};
+NoallocSlot g_noalloc_slots[64];
+
+unsigned char *noalloc_scratch(int device, cudaError_t &err) {
+  if (device < 0 || device >= 64) {
+    err = cudaErrorInvalidDevice;
+    return nullptr;
+  }
+  NoallocSlot &slot = g_noalloc_slots[device];
+  std::call_once(slot.once, [&]() {
+    void *p = nullptr;
+    slot.err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    slot.ptr = slot.err == cudaSuccess ? static_cast<unsigned char *>(p) : nullptr;
+  });
+  err = slot.err;
+  return slot.ptr;
+}
+}  // namespace
+
+extern "C" int ccs_run_device_noalloc(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t *d_status,
+                                      double *d_omc, uint32_t *d_steps, uint32_t *d_visits, void *stream,
+                                      ccs_stats *stats) {
+  if (!c) return CCS_ERR_INVALID;
+  if (!c->have_target) return fail(c, CCS_ERR_INVALID, "no target set");
+  if (n == 0) return CCS_OK;
+  if (n > NOALLOC_MAX_TRAJ)
+    return fail(c, CCS_ERR_INVALID,
+                "ccs_run_device_noalloc: %zu trajectories exceed the maximum of %zu per call (the fixed scratch "
+                "holds the park buffer for that many); split the run or use ccs_run_device",
+                n, NOALLOC_MAX_TRAJ);
+  if (!d_rnd || !d_status || !d_omc || stride < n) return fail(c, CCS_ERR_INVALID, "bad device buffers");
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
+  cudaError_t serr = cudaSuccess;
+  unsigned char *base = noalloc_scratch(c->device, serr);
+  if (!base) return fail(c, CCS_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(serr));
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  unsigned long long *work = reinterpret_cast<unsigned long long *>(base);  // [0] counter [1..7] stats [8] clock [9..10] park
+  int *error = reinterpret_cast<int *>(base + 11 * sizeof(unsigned long long));
+  KParams *kparams = reinterpret_cast<KParams *>(base + NOALLOC_HEADER_BYTES);
+  void *park = base + NOALLOC_HEADER_BYTES + NOALLOC_PARAMS_BYTES;
+  // lanes per force evaluation: the configured or already tuned value (no autotuning here)
+  const int G = c->p.lanes_per_traj > 0 ? c->p.lanes_per_traj : (c->tuned_G ? c->tuned_G : 32);
+  const int block = BLOCK;
+  KParams k = base_params(c);
+  k.rnd = d_rnd;
+  k.rnd_stride = stride;
+  k.ntraj = n;
+  k.status = d_status;
+  k.omc = d_omc;
+  k.steps = d_steps;
+  k.visits = d_visits;
+  k.order = nullptr;  // index order (the processing order never changes a result)
+  k.work = work;
+  k.stats = work + 1;
+  k.error = error;
+  k.park = park;
+  k.park_cap = std::min<size_t>(n, NOALLOC_PARK_CAP);
+  k.park_steps = c->p.park_steps ? c->p.park_steps : 4096u;
+  k.park_count = work + 9;
+  k.park_next = work + 10;
+  // everything that must start at zero: counters, statistics, park counters, error flag
+  CK(cudaMemsetAsync(base, 0, NOALLOC_HEADER_BYTES, s));
+  read_globaltimer<<<1, 1, 0, s>>>(work + 8);
+  CK(cudaGetLastError());
+  unsigned long long now = 0;
+  CK(cudaMemcpyAsync(&now, work + 8, sizeof now, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const double wd = c->p.watchdog_s > 0 ? c->p.watchdog_s : 600.0;
+  k.deadline_ns = now + (unsigned long long)(wd * 1e9);
+  copy_params_kernel<<<1, 1, 0, s>>>(k, kparams);
+  CK(cudaGetLastError());
+  KernelFn fn = pick_traj(c, G);
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, 0));
+  size_t grid = (size_t)std::max(per_sm, 1) * c->sm_count;
+  grid = std::min(grid, std::max<size_t>(1, (n + block - 1) / block));
+  fn<<<(unsigned)grid, block, 0, s>>>(k, kparams);
+  CK(cudaGetLastError());
+  KernelFn rfn = pick_resume(c);
+  int rper_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, RBLOCK, 0));
+  rfn<<<(unsigned)((size_t)std::max(rper_sm, 1) * c->sm_count), RBLOCK, 0, s>>>(k, kparams);
+  CK(cudaGetLastError());
+  if (stats) {
+    unsigned long long h[7];
+    int herr = 0;
+    CK(cudaMemcpyAsync(h, work + 1, sizeof h, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&herr, error, sizeof herr, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    std::memset(stats, 0, sizeof *stats);
+    stats->ntraj = n;
+    stats->nfree = h[0]; stats->nscatter = h[1]; stats->nlost = h[2]; stats->ncapped = h[3];
+    stats->steps = h[4]; stats->visits = h[5]; stats->parked = h[6];
+    stats->lanes_per_traj = G; stats->block_size = block; stats->grid_size = (int32_t)grid;
+    if (herr) return fail(c, CCS_ERR_TIMEOUT, "device watchdog expired");
+  }
+  return CCS_OK;
+}

@@ -73,7 +73,7 @@ class CcsInfo(ctypes.Structure):
 EXPORTS = ["ccs_version", "ccs_create", "ccs_destroy", "ccs_params_default", "ccs_set_target",
            "ccs_set_params", "ccs_run", "ccs_run_device", "ccs_sync_stats", "ccs_eval_site_forces",
            "ccs_eval_setup", "ccs_get_info", "ccs_status_string", "ccs_last_error",
-           "ccs_measure_fp32_peak"]
+           "ccs_measure_fp32_peak", "ccs_run_device_noalloc"]
 
 _LIB = None
 
@@ -107,6 +107,7 @@ def load_library(path=LIB_PATH):
     L.ccs_last_error.argtypes = [vp]
     L.ccs_last_error.restype = ctypes.c_char_p
     L.ccs_measure_fp32_peak.argtypes = [i32, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+    L.ccs_run_device_noalloc.argtypes = [vp, sz, vp, sz, vp, vp, vp, vp, vp, ctypes.POINTER(CcsStats)]
     if path == LIB_PATH:
         _LIB = L
     return L
@@ -205,6 +206,17 @@ class Engine:
         self._check(self._L.ccs_run_device(self._h, n, d_rnd, stride, d_status, d_omc,
                                            d_steps or None, d_visits or None, stream or None),
                     "ccs_run_device")
+
+    def run_device_noalloc(self, n, d_rnd, stride, d_status, d_omc, d_steps=0, d_visits=0, stream=0,
+                           want_stats=True):
+        """ccs_run_device_noalloc: the same run with all scratch in the library's static
+        device array (no device allocation); returns the statistics when asked."""
+        st = CcsStats() if want_stats else None
+        self._check(self._L.ccs_run_device_noalloc(self._h, n, d_rnd, stride, d_status, d_omc,
+                                                   d_steps or None, d_visits or None, stream or None,
+                                                   ctypes.byref(st) if st is not None else None),
+                    "ccs_run_device_noalloc")
+        return st.as_dict() if st is not None else None
 
     def sync_stats(self):
         st = CcsStats()
