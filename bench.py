@@ -199,6 +199,8 @@ def main():
     ap.add_argument("--config", default="globule_n2", choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ntraj", type=int, default=0,
+                    help="trajectories per step (default: the workload's 3e5); smaller values are for profiling")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -226,7 +228,7 @@ def main():
     d = tempfile.mkdtemp(prefix=f"bench_{rank}_")
     json_path = make_workload(args.config, d)
     S = H.System(json_path)
-    n = cfg["ntraj"]
+    n = args.ntraj if args.ntraj > 0 else cfg["ntraj"]
     seed = S.info["seed"] + rank  # each rank its own trajectories
     rnd_host = S.predraw(n, seed=seed)
     eng = S.engine(device=local)

@@ -1125,17 +1125,17 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
   if (threadIdx.x == 7 && blk[7]) atomicAdd(&kp.stats[6], blk[7]);
 }
 
-// Warp pass: parked trajectories resume one per CTA (all RBLOCK threads hold
+// Warp pass: parked trajectories resume one per CTA (all NT threads hold
 // the same state; the force phase is block-cooperative).
-constexpr int RBLOCK = 128;  // threads per trajectory in the warp pass
+constexpr int RBLOCK = 64;  // default threads per trajectory in the warp pass
 
-template <typename T, int GAS, bool HASQ>
-__global__ void __launch_bounds__(RBLOCK) resume_kernel(KParams kp, const KParams *__restrict__ kpg) {
+template <typename T, int GAS, bool HASQ, int NT>
+__global__ void __launch_bounds__(NT) resume_kernel(KParams kp, const KParams *__restrict__ kpg) {
   using S = Sites<GAS>;
   constexpr int NS = S::NS;
   constexpr int NV = 4 * NS + 9;
-  __shared__ int sm_end[RBLOCK], sm_del[RBLOCK], sm_wsum[RBLOCK / 32];
-  __shared__ T sm_red[(RBLOCK / 32 + 1) * NV];
+  __shared__ int sm_end[NT], sm_del[NT], sm_wsum[NT / 32];
+  __shared__ T sm_red[(NT / 32 + 1) * NV];
   __shared__ unsigned long long blk[8];
   __shared__ unsigned long long sm_idx;
   if (threadIdx.x < 8) blk[threadIdx.x] = 0ull;
@@ -1169,7 +1169,7 @@ __global__ void __launch_bounds__(RBLOCK) resume_kernel(KParams kp, const KParam
         bool act[NS];
 #pragma unroll
         for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
-        eval_forces_block<T, RBLOCK, GAS, HASQ>(kp, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
+        eval_forces_block<T, NT, GAS, HASQ>(kp, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
                                               tid, sm_end, sm_del, sm_wsum, sm_red);
       } else {
 #pragma unroll

@@ -153,7 +153,10 @@ void vel_table(double m_amu, double T, std::vector<double> &V, std::vector<doubl
 }
 
 using KernelFn = void (*)(KParams, const KParams *);
-template <typename T, int GAS, bool HASQ> KernelFn resume_ptr() { return resume_kernel<T, GAS, HASQ>; }
+template <typename T, int GAS, bool HASQ> KernelFn resume_ptr(int nt) {
+  return nt == 32 ? resume_kernel<T, GAS, HASQ, 32> : nt == 64 ? resume_kernel<T, GAS, HASQ, 64>
+                                                               : resume_kernel<T, GAS, HASQ, 128>;
+}
 using ForceFn = void (*)(KParams, int, size_t, const double *, double *, double *, uint32_t *);
 
 template <typename T, int G, int GAS, bool HASQ> KernelFn traj_ptr() { return traj_kernel<T, G, GAS, HASQ>; }
@@ -196,17 +199,24 @@ KernelFn pick_traj(const ccs_ctx *c, int G) {
   return c->p.precision == CCS_PREC_FP64 ? pick_traj_t<double>(gas, hasq, g_index(G))
                                          : pick_traj_t<float>(gas, hasq, g_index(G));
 }
+// threads per trajectory in the warp pass
+int resume_threads(const ccs_ctx *c) {
+  const int b = c->p.resume_block;
+  return (b == 32 || b == 64 || b == 128) ? b : RBLOCK;
+}
+
 KernelFn pick_resume(const ccs_ctx *c) {
   const int gas = gas_kind(c->p.gas);
   const bool hasq = c->coul_on || c->dip_on;
+  const int nt = resume_threads(c);
   if (c->p.precision == CCS_PREC_FP64) {
-    if (gas == GAS_ATOM) return hasq ? resume_ptr<double, GAS_ATOM, true>() : resume_ptr<double, GAS_ATOM, false>();
-    if (gas == GAS_N2) return hasq ? resume_ptr<double, GAS_N2, true>() : resume_ptr<double, GAS_N2, false>();
-    return hasq ? resume_ptr<double, GAS_CO2, true>() : resume_ptr<double, GAS_CO2, false>();
+    if (gas == GAS_ATOM) return hasq ? resume_ptr<double, GAS_ATOM, true>(nt) : resume_ptr<double, GAS_ATOM, false>(nt);
+    if (gas == GAS_N2) return hasq ? resume_ptr<double, GAS_N2, true>(nt) : resume_ptr<double, GAS_N2, false>(nt);
+    return hasq ? resume_ptr<double, GAS_CO2, true>(nt) : resume_ptr<double, GAS_CO2, false>(nt);
   }
-  if (gas == GAS_ATOM) return hasq ? resume_ptr<float, GAS_ATOM, true>() : resume_ptr<float, GAS_ATOM, false>();
-  if (gas == GAS_N2) return hasq ? resume_ptr<float, GAS_N2, true>() : resume_ptr<float, GAS_N2, false>();
-  return hasq ? resume_ptr<float, GAS_CO2, true>() : resume_ptr<float, GAS_CO2, false>();
+  if (gas == GAS_ATOM) return hasq ? resume_ptr<float, GAS_ATOM, true>(nt) : resume_ptr<float, GAS_ATOM, false>(nt);
+  if (gas == GAS_N2) return hasq ? resume_ptr<float, GAS_N2, true>(nt) : resume_ptr<float, GAS_N2, false>(nt);
+  return hasq ? resume_ptr<float, GAS_CO2, true>(nt) : resume_ptr<float, GAS_CO2, false>(nt);
 }
 ForceFn pick_force(const ccs_ctx *c, int G) {
   const int gas = gas_kind(c->p.gas);
@@ -394,9 +404,10 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   // warp pass over the parked trajectories (exits at once when none were parked)
   KernelFn rfn = pick_resume(c);
   int rper_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, RBLOCK, 0));
+  const int rnt = resume_threads(c);
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, rnt, 0));
   if (rper_sm < 1) rper_sm = 1;
-  rfn<<<(unsigned)((size_t)rper_sm * c->sm_count), RBLOCK, 0, s>>>(k, c->d_kparams);
+  rfn<<<(unsigned)((size_t)rper_sm * c->sm_count), rnt, 0, s>>>(k, c->d_kparams);
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev[7], s));
   c->last.grid_size = (int32_t)grid;
@@ -1013,8 +1024,9 @@ extern "C" int ccs_run_device_noalloc(ccs_ctx *c, size_t n, const double *d_rnd,
   CK(cudaGetLastError());
   KernelFn rfn = pick_resume(c);
   int rper_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, RBLOCK, 0));
-  rfn<<<(unsigned)((size_t)std::max(rper_sm, 1) * c->sm_count), RBLOCK, 0, s>>>(k, kparams);
+  const int rnt = resume_threads(c);
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, rnt, 0));
+  rfn<<<(unsigned)((size_t)std::max(rper_sm, 1) * c->sm_count), rnt, 0, s>>>(k, kparams);
   CK(cudaGetLastError());
   if (stats) {
     unsigned long long h[7];

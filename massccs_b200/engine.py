@@ -33,6 +33,7 @@ class CcsParams(ctypes.Structure):
         ("max_steps_per_try", ctypes.c_uint32),
         ("watchdog_s", ctypes.c_double),
         ("schedule", ctypes.c_int32), ("park_steps", ctypes.c_uint32),
+        ("resume_block", ctypes.c_int32),
     ]
 
 

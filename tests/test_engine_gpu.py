@@ -121,3 +121,30 @@ def _paired_ccs_ok(bmax, ref, out):
     w_ref = a[ok].mean()
     se = d.std(ddof=1) / np.sqrt(len(d))
     assert abs(d.mean()) <= max(0.005 * w_ref, 4 * se), (d.mean(), se, w_ref)
+
+
+# A low park threshold sends most trajectories through both passes (lane
+# pass, then the warp pass after 64 steps): the hand-over must not change a
+# result, whatever the warp pass's threads per trajectory.
+PASSES = [("c60.xyz", "He", 4, 1500), ("04_1ubq_charge_4e_min.pqr", "N2", 6, 300), ("c60.xyz", "CO2", 4, 400)]
+
+
+@pytest.mark.parametrize("target,gas,ft,n", PASSES)
+@pytest.mark.parametrize("resume_block", [0, 32, 64])
+def test_trajectories_fp64_through_both_passes(oracle, target, gas, ft, n, resume_block):
+    s, ref, out = _paired(oracle, target, gas, ft, n, prec=1, park_steps=64, resume_block=resume_block)
+    assert out["stats"]["parked"] > n // 4
+    same = out["status"] == ref["status"]
+    assert same.mean() >= 0.97
+    close = same & (np.abs(out["one_minus_cos"] - ref["one_minus_cos"]) <= 1e-7)
+    assert close.mean() >= 0.97, close.mean()
+    assert (out["steps"] == ref["steps"]).mean() >= 0.97
+
+
+@pytest.mark.parametrize("target,gas,ft,n", PASSES)
+@pytest.mark.parametrize("resume_block", [32, 128])
+def test_trajectories_fp32_through_both_passes(oracle, target, gas, ft, n, resume_block):
+    s, ref, out = _paired(oracle, target, gas, ft, n, prec=0, park_steps=64, resume_block=resume_block)
+    assert out["stats"]["parked"] > n // 4
+    assert (out["status"] == ref["status"]).mean() >= 0.97
+    _paired_ccs_ok(s.params["bmax"], ref, out)
