@@ -148,3 +148,21 @@ def test_trajectories_fp32_through_both_passes(oracle, target, gas, ft, n, resum
     assert out["stats"]["parked"] > n // 4
     assert (out["status"] == ref["status"]).mean() >= 0.97
     _paired_ccs_ok(s.params["bmax"], ref, out)
+
+
+def test_watchdog_expiry_is_an_error_and_the_context_survives(oracle):
+    """A device wall-time budget far below the run's length: every CTA drains
+    at its next check, the call returns CCS_ERR_TIMEOUT, and the same context
+    runs normally afterwards (no fault, no hang: the deadline is polled)."""
+    from massccs_b200 import engine as E
+    s = oracle_system(oracle, target="04_1ubq_charge_4e_min.pqr", gas="N2", ft=6, nprobe=3000)
+    rnd = s.predraw(3000)
+    eng = engine_for(s, precision=0, lanes_per_traj=32, watchdog_s=1e-3)
+    with pytest.raises(E.CcsError, match="watchdog"):
+        eng.run(rnd)
+    eng.set_params(E.params_from_system(s.params, precision=0, lanes_per_traj=32))
+    t = s.target()
+    eng.set_target(t["x"], t["y"], t["z"], t["q"], t["eps"], t["sig"])
+    out = eng.run(rnd[:, :400])
+    assert out["stats"]["ncapped"] == 0
+    assert (out["status"] <= 1).mean() > 0.9

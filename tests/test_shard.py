@@ -1,0 +1,73 @@
+"""Sharding of one run over ranks (CPU, gloo, world sizes 2 and 3).
+
+Each rank runs only its contiguous range of trajectories (here through the
+oracle, on its own columns of the pre-draw); the gathered results and the
+fixed-order reduction must equal the single-process run exactly, for even
+and uneven splits.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from helpers import input_dict, workdir, write_input
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, json_path, out_dir):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        from oracle import pyoracle
+        from massccs_b200 import shard
+        s = pyoracle.OracleSystem(json_path)
+        info = s.params
+        n = info["nprobe"] * info["niter"]
+        rnd = np.ascontiguousarray(shard.local_rnd(s.predraw(n), rank, world))
+        res = s.run(rnd, nthreads=1)
+        red = shard.sharded_ccs(res["status"], res["one_minus_cos"], info["niter"], info["nprobe"], info["bmax"])
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), omega=red["omega"], ccs=red["ccs"], err=red["err"],
+                 nfree=red["nfree"], nscatter=red["nscatter"], nlost=red["nlost"])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_shard_range_covers_every_trajectory():
+    from massccs_b200 import shard
+    for n in (0, 1, 7, 300, 300001):
+        for w in (1, 2, 3, 8):
+            spans = [shard.shard_range(n, r, w) for r in range(w)]
+            assert spans[0][0] == 0 and spans[-1][1] == n
+            assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+            sizes = [e - s for s, e in spans]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        shard.shard_range(10, 2, 2)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_run_equals_single_process(oracle, world, tmp_path):
+    import torch.multiprocessing as mp
+    d = workdir()
+    p = write_input(d, input_dict("c60.xyz", "He", 4, nprobe=40, niter=5))
+    s = oracle.OracleSystem(p)
+    n = 200
+    full = s.run(s.predraw(n), nthreads=1)
+    ref = oracle.reduce(5, 40, full["status"], full["one_minus_cos"], s.params["bmax"])
+    mp.start_processes(_worker, args=(world, _free_port(), p, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    for r in range(world):
+        got = np.load(tmp_path / f"rank{r}.npz")
+        np.testing.assert_array_equal(got["omega"], ref["omega"])
+        np.testing.assert_array_equal(got["nfree"], ref["nfree"])
+        assert float(got["ccs"]) == ref["ccs"] and float(got["err"]) == ref["err"]
