@@ -356,21 +356,59 @@ __device__ __forceinline__ void eval_forces(const KParams &kp, const T (&p)[GasS
   visits += nvis;
 }
 
+// Sum of P values over the 32 lanes of a warp, scattered: a reduce-scatter
+// butterfly in which each exchange sends half of the values still held, so
+// the warp spends 2P - 1 shuffles (not 5P).  Afterwards lane l holds in v[0]
+// the warp sum of value index (l >> (5 - log2 P)); lanes that share an index
+// hold identical bits (each pairwise sum is commutative).
+template <int O, int C, int P, typename T> __device__ __forceinline__ void rs_level(T (&v)[P], int lane) {
+  if constexpr (C == 1) {
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], O);
+  } else {
+    constexpr int H = C / 2;
+    const bool up = (lane & O) != 0;
+#pragma unroll
+    for (int i = 0; i < H; i++) {
+      const T send = up ? v[i] : v[i + H];
+      const T keep = up ? v[i + H] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+    }
+  }
+  if constexpr (O > 1) rs_level<O / 2, (C == 1 ? 1 : C / 2), P>(v, lane);
+}
+template <int P, typename T> __device__ __forceinline__ void warp_reduce_scatter(T (&v)[P], int lane) {
+  static_assert(P >= 1 && P <= 32 && (P & (P - 1)) == 0, "P must be a power of two <= 32");
+  rs_level<16, P, P>(v, lane);
+}
+template <int P> constexpr int log2_of() { return P <= 1 ? 0 : 1 + log2_of<P / 2>(); }
+
+// values reduced per force evaluation: per site f (3) and U, then the field
+// (3) and its gradient (6) at the dipole site; padded to a power of two
+template <int GAS> struct RedShape {
+  static constexpr int NV = 4 * GasShape<GAS>::NS + 9;
+  static constexpr int P = NV <= 16 ? 16 : 32;
+};
+constexpr int LCAP = 1024;  // candidate-list entries staged in shared memory per chunk
+
 // Block-cooperative site forces for the warp pass: all NT threads of a CTA
-// evaluate one probe configuration.  Columns are split over the threads, the
-// run lengths are scanned block-wide, every thread visits candidates t, t+NT,
-// ... (two per iteration for instruction-level parallelism), and the sums are
-// reduced per warp (xor shuffles) and then across warps in shared memory in
-// a fixed order, so every thread ends with identical bits.
+// evaluate one probe configuration.  Columns are split over the threads and
+// their z-runs are flattened into a candidate list in shared memory (an
+// exclusive block scan of the run lengths gives every run its place; chunks
+// of LCAP entries), so each thread reads candidate t, t+NT, ... directly, two
+// per iteration for instruction-level parallelism.  The sums are reduced per
+// warp with a reduce-scatter butterfly and then across warps in shared memory
+// in a fixed order, so every thread ends with identical bits.
+//   sm_list: LCAP ints; sm_wsum: NT/32 ints; sm_red: (NT/32 + 1) * RedShape<GAS>::P values
 template <typename T, int NT, int GAS, bool HASQ>
 __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
                                                   const bool (&act)[GasShape<GAS>::NS], const T (&cen)[3],
                                                   T off, T (&f)[GasShape<GAS>::NS][3],
                                                   T (&U)[GasShape<GAS>::NS], uint32_t &visits, int tid,
-                                                  int *sm_end, int *sm_del, int *sm_wsum, T *sm_red) {
+                                                  int *sm_list, int *sm_wsum, T *sm_red) {
   constexpr int NS = GasShape<GAS>::NS;
   constexpr int NW = NT / 32;
-  constexpr int NV = 4 * NS + 9;
+  constexpr int NV = RedShape<GAS>::NV;
+  constexpr int P = RedShape<GAS>::P;
   const int lane = tid & 31, w = tid >> 5;
   Acc<T, NS> acc;
   acc.zero();
@@ -431,7 +469,7 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
             }
           }
         }
-        // block-wide inclusive scan of the run lengths
+        // block-wide exclusive scan of the run lengths
         int incl = len;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -447,38 +485,33 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
           wofs += k < w ? ws : 0;
           total += ws;
         }
-        incl += wofs;
-        sm_end[tid] = incl;
-        sm_del[tid] = b - (incl - len);
-        __syncthreads();
-        if (total > 0) {
-          int r = 0, cur_end = sm_end[0], cur_del = sm_del[0];
-          int r2 = 0, cur_end2 = cur_end, cur_del2 = cur_del;
+        const int excl = incl + wofs - len;
+        for (int cs = 0; cs < total; cs += LCAP) {
+          // this thread's run, as far as it falls into the chunk [cs, cs + LCAP)
+          const int lo = max(excl, cs), hi = min(excl + len, cs + LCAP);
+          for (int q = lo; q < hi; q++) sm_list[q - cs] = b + (q - excl);
+          __syncthreads();
+          const int m = min(LCAP, total - cs);
           int t = tid;
-          for (; t + NT < total; t += 2 * NT) {
-            while (t >= cur_end) { ++r; cur_end = sm_end[r]; cur_del = sm_del[r]; }
-            const int t2 = t + NT;
-            if (r2 < r) { r2 = r; cur_end2 = cur_end; cur_del2 = cur_del; }
-            while (t2 >= cur_end2) { ++r2; cur_end2 = sm_end[r2]; cur_del2 = sm_del[r2]; }
-            const Atom<T> a1 = load_atom<T, GAS>(kp, t + cur_del);
-            const Atom<T> a2 = load_atom<T, GAS>(kp, t2 + cur_del2);
+          for (; t + NT < m; t += 2 * NT) {
+            const Atom<T> a1 = load_atom<T, GAS>(kp, sm_list[t]);
+            const Atom<T> a2 = load_atom<T, GAS>(kp, sm_list[t + NT]);
             visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
             visit_atom<T, GAS, HASQ>(kp, p, act, a2, acc);
-            r = r2; cur_end = cur_end2; cur_del = cur_del2;
           }
-          if (t < total) {
-            while (t >= cur_end) { ++r; cur_end = sm_end[r]; cur_del = sm_del[r]; }
-            const Atom<T> a1 = load_atom<T, GAS>(kp, t + cur_del);
+          if (t < m) {
+            const Atom<T> a1 = load_atom<T, GAS>(kp, sm_list[t]);
             visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
           }
-          nvis += (uint32_t)total;
+          __syncthreads();  // the list and sm_wsum are rewritten next
         }
-        __syncthreads();
+        if (total == 0) __syncthreads();  // sm_wsum is rewritten next (block-uniform branch)
+        nvis += (uint32_t)total;
       }
     }
   }
-  // two-level reduction in a fixed order
-  T v[NV];
+  // reduce-scatter per warp, then the warps in a fixed order
+  T v[P];
 #pragma unroll
   for (int s = 0; s < NS; s++) {
     v[4 * s] = acc.f[s][0]; v[4 * s + 1] = acc.f[s][1]; v[4 * s + 2] = acc.f[s][2]; v[4 * s + 3] = acc.U[s];
@@ -488,32 +521,35 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
 #pragma unroll
   for (int k = 0; k < 6; k++) v[4 * NS + 3 + k] = acc.G[k];
 #pragma unroll
-  for (int k = 0; k < NV; k++) v[k] = group_sum<32>(v[k], 0xffffffffu);
+  for (int k = NV; k < P; k++) v[k] = T(0);
+  warp_reduce_scatter<P>(v, lane);
+  constexpr int SH = 5 - log2_of<P>();  // lanes per value index = 1 << SH
+  T out[NV];
   if constexpr (NW > 1) {
-    if (lane == 0) {
-#pragma unroll
-      for (int k = 0; k < NV; k++) sm_red[w * NV + k] = v[k];
-    }
+    if ((lane & ((1 << SH) - 1)) == 0) sm_red[w * P + (lane >> SH)] = v[0];
     __syncthreads();
     if (tid < NV) {  // one thread per value sums the warps in a fixed order
       T sum = sm_red[tid];
 #pragma unroll
-      for (int q = 1; q < NW; q++) sum += sm_red[q * NV + tid];
-      sm_red[NW * NV + tid] = sum;
+      for (int q = 1; q < NW; q++) sum += sm_red[q * P + tid];
+      sm_red[NW * P + tid] = sum;
     }
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < NV; k++) v[k] = sm_red[NW * NV + k];
+    for (int k = 0; k < NV; k++) out[k] = sm_red[NW * P + k];
     __syncthreads();
+  } else {
+#pragma unroll
+    for (int k = 0; k < NV; k++) out[k] = __shfl_sync(0xffffffffu, v[0], k << SH);
   }
 #pragma unroll
   for (int s = 0; s < NS; s++) {
-    f[s][0] = v[4 * s]; f[s][1] = v[4 * s + 1]; f[s][2] = v[4 * s + 2]; U[s] = v[4 * s + 3];
+    f[s][0] = out[4 * s]; f[s][1] = out[4 * s + 1]; f[s][2] = out[4 * s + 2]; U[s] = out[4 * s + 3];
   }
   if (HASQ && kp.dip_on) {
     constexpr int d = GasShape<GAS>::DIP;
     const T al = T(kp.alpha);
-    const T *E = v + 4 * NS, *Gr = v + 4 * NS + 3;
+    const T *E = out + 4 * NS, *Gr = out + 4 * NS + 3;
     f[d][0] += al * (E[0] * Gr[0] + E[1] * Gr[3] + E[2] * Gr[4]);
     f[d][1] += al * (E[0] * Gr[3] + E[1] * Gr[1] + E[2] * Gr[5]);
     f[d][2] += al * (E[0] * Gr[4] + E[1] * Gr[5] + E[2] * Gr[2]);
@@ -1133,9 +1169,8 @@ template <typename T, int GAS, bool HASQ, int NT>
 __global__ void __launch_bounds__(NT) resume_kernel(KParams kp, const KParams *__restrict__ kpg) {
   using S = Sites<GAS>;
   constexpr int NS = S::NS;
-  constexpr int NV = 4 * NS + 9;
-  __shared__ int sm_end[NT], sm_del[NT], sm_wsum[NT / 32];
-  __shared__ T sm_red[(NT / 32 + 1) * NV];
+  __shared__ int sm_list[LCAP], sm_wsum[NT / 32];
+  __shared__ T sm_red[(NT / 32 + 1) * RedShape<GAS>::P];
   __shared__ unsigned long long blk[8];
   __shared__ unsigned long long sm_idx;
   if (threadIdx.x < 8) blk[threadIdx.x] = 0ull;
@@ -1170,7 +1205,7 @@ __global__ void __launch_bounds__(NT) resume_kernel(KParams kp, const KParams *_
 #pragma unroll
         for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
         eval_forces_block<T, NT, GAS, HASQ>(kp, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
-                                              tid, sm_end, sm_del, sm_wsum, sm_red);
+                                              tid, sm_list, sm_wsum, sm_red);
       } else {
 #pragma unroll
         for (int s = 0; s < NS; s++) fs[s][0] = fs[s][1] = fs[s][2] = Us[s] = T(0);
