@@ -162,6 +162,10 @@ template <int G, typename T> __device__ __forceinline__ T group_sum(T v, unsigne
 }
 
 // One target atom against every active site (the pair terms of Force.cpp).
+// Branch-free over the cutoff tests: every term is computed and the ones
+// outside their cutoff are selected away (a select, never a multiply, so an
+// infinite or NaN term of an excluded pair cannot leak into the sums).  The
+// lanes of a warp therefore never diverge on a pair's distance.
 template <typename T, int GAS, bool HASQ>
 __device__ __forceinline__ void visit_atom(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
                                            const bool (&act)[GasShape<GAS>::NS], const Atom<T> &a,
@@ -174,42 +178,41 @@ __device__ __forceinline__ void visit_atom(const KParams &kp, const T (&p)[GasSh
     const T dx = p[s][0] - a.x, dy = p[s][1] - a.y, dz = p[s][2] - a.z;
     const T r2 = dx * dx + dy * dy + dz * dz;
     const int lj = site_lj<GAS>(s);
-    const bool in_lj = lj != 0 && r2 < rlj2;
-    const bool in_c = HASQ && r2 < rc2;
-    if (!(in_lj || in_c)) continue;
     const T ir = Real<T>::rsq(r2);
     const T ir2 = ir * ir;
-    if (in_lj) {
+    if (lj != 0) {
       // Force.cpp:83-102: U = A/r^12 - B/r^6 - (A/rc^12 - B/rc^6), F = (12A/r^12 - 6B/r^6)/r^2 * d
+      const bool in_lj = r2 < rlj2;
       const T A = lj == 2 ? a.Ac : a.A, B = lj == 2 ? a.Bc : a.B;
       const T ir6 = ir2 * ir2 * ir2;
-      acc.U[s] += ir6 * (A * ir6 - B) - (A * T(kp.rc12inv) - B * T(kp.rc6inv));
-      const T fl = ir6 * (T(12) * A * ir6 - T(6) * B) * ir2;
+      const T u = ir6 * (A * ir6 - B) - (A * T(kp.rc12inv) - B * T(kp.rc6inv));
+      const T fl = in_lj ? ir6 * (T(12) * A * ir6 - T(6) * B) * ir2 : T(0);
+      acc.U[s] += in_lj ? u : T(0);
       acc.f[s][0] += fl * dx; acc.f[s][1] += fl * dy; acc.f[s][2] += fl * dz;
     }
     if constexpr (HASQ) {
-      if (in_c) {
-        const T ir3 = ir * ir2;
-        if (site_coul<GAS>(s) && kp.coul_on) {
-          // Force.cpp:671-683: U = k qi qj (1/r - 3/(2rc) + r^2/(2rc^3)), F = k qi qj (1/r^3 - 1/rc^3) d
-          const T kq = T(KCOUL * kp.q_site[s]) * a.q;
-          acc.U[s] += kq * (ir - T(kp.c1) + T(kp.c2) * r2);
-          const T fc = kq * (ir3 - T(kp.rc3inv));
-          acc.f[s][0] += fc * dx; acc.f[s][1] += fc * dy; acc.f[s][2] += fc * dz;
-        }
-        if (s == GasShape<GAS>::DIP && kp.dip_on) {
-          // Force.cpp:393-426: E += q (1/r^3 - 1/rc^3) d ; dE_ab += q (1/r^3 - 1/rc^3) delta_ab - 3 q d_a d_b / r^5
-          const T sq = a.q * (ir3 - T(kp.rc3inv));
-          const T tq = T(-3) * a.q * ir3 * ir2;
-          acc.E[0] += sq * dx; acc.E[1] += sq * dy; acc.E[2] += sq * dz;
-          const T tx = tq * dx, ty = tq * dy;
-          acc.G[0] += sq + tx * dx;
-          acc.G[1] += sq + ty * dy;
-          acc.G[2] += sq + tq * dz * dz;
-          acc.G[3] += tx * dy;
-          acc.G[4] += tx * dz;
-          acc.G[5] += ty * dz;
-        }
+      const bool in_c = r2 < rc2;
+      const T ir3 = ir * ir2;
+      if (site_coul<GAS>(s) && kp.coul_on) {
+        // Force.cpp:671-683: U = k qi qj (1/r - 3/(2rc) + r^2/(2rc^3)), F = k qi qj (1/r^3 - 1/rc^3) d
+        const T kq = T(KCOUL * kp.q_site[s]) * a.q;
+        const T u = kq * (ir - T(kp.c1) + T(kp.c2) * r2);
+        const T fc = in_c ? kq * (ir3 - T(kp.rc3inv)) : T(0);
+        acc.U[s] += in_c ? u : T(0);
+        acc.f[s][0] += fc * dx; acc.f[s][1] += fc * dy; acc.f[s][2] += fc * dz;
+      }
+      if (s == GasShape<GAS>::DIP && kp.dip_on) {
+        // Force.cpp:393-426: E += q (1/r^3 - 1/rc^3) d ; dE_ab += q (1/r^3 - 1/rc^3) delta_ab - 3 q d_a d_b / r^5
+        const T sq = in_c ? a.q * (ir3 - T(kp.rc3inv)) : T(0);
+        const T tq = in_c ? T(-3) * a.q * ir3 * ir2 : T(0);
+        acc.E[0] += sq * dx; acc.E[1] += sq * dy; acc.E[2] += sq * dz;
+        const T tx = tq * dx, ty = tq * dy;
+        acc.G[0] += sq + tx * dx;
+        acc.G[1] += sq + ty * dy;
+        acc.G[2] += sq + tq * dz * dz;
+        acc.G[3] += tx * dy;
+        acc.G[4] += tx * dz;
+        acc.G[5] += ty * dz;
       }
     }
   }
@@ -255,7 +258,9 @@ __device__ __forceinline__ void eval_forces(const KParams &kp, const T (&p)[GasS
     const T fx = fmax(cx - T(kp.bb_lo[0]), T(kp.bb_hi[0]) - cx);
     const T fy = fmax(cy - T(kp.bb_lo[1]), T(kp.bb_hi[1]) - cy);
     const T fz = fmax(cz - T(kp.bb_lo[2]), T(kp.bb_hi[2]) - cz);
-    if (fx * fx + fy * fy + fz * fz <= R * R) {
+    if ((G > 1 && kp.natoms <= 2 * G) || fx * fx + fy * fy + fz * fz <= R * R) {
+      // the whole target inside the reach sphere, or a target of at most two
+      // atoms per lane of the group: every atom is a candidate
       for (int ai = g; ai < kp.natoms; ai += G) {
         const Atom<T> a = load_atom<T, GAS>(kp, ai);
         visit_atom<T, GAS, HASQ>(kp, p, act, a, acc);
@@ -388,23 +393,156 @@ template <int GAS> struct RedShape {
   static constexpr int NV = 4 * GasShape<GAS>::NS + 9;
   static constexpr int P = NV <= 16 ? 16 : 32;
 };
-constexpr int LCAP = 1024;  // candidate-list entries staged in shared memory per chunk
+constexpr int LCAP = 2048;  // candidate-list entries kept in shared memory per CTA
+constexpr float LSKIN = 1.0f;  // A: the list's margin; reused while the probe moves less
+
+// Column (i,j) number cidx of the ncol columns meeting the sphere of radius Rr
+// around c: its z-run of atoms [b, b + len) clipped to the sphere.
+template <typename T>
+__device__ __forceinline__ void column_run(const KParams &kp, int cidx, int ncol, int i0, int j0, int nj,
+                                           float inv_nj, T cx, T cy, T cz, T Rr, int &b, int &len) {
+  b = 0;
+  len = 0;
+  if (cidx >= ncol) return;
+  const T ih = T(kp.inv_h), h = T(kp.h), ox = T(kp.ox), oy = T(kp.oy), oz = T(kp.oz);
+  const int di = (int)(((float)cidx + 0.5f) * inv_nj);  // exact: cidx < 2^20
+  const int i = i0 + di, j = j0 + (cidx - di * nj);
+  const T xlo = ox + T(i) * h, ylo = oy + T(j) * h;
+  const T dxc = fmax(fmax(xlo - cx, cx - (xlo + h)), T(0));
+  const T dyc = fmax(fmax(ylo - cy, cy - (ylo + h)), T(0));
+  const T rem = Rr * Rr - dxc * dxc - dyc * dyc;
+  if (rem < T(0)) return;
+  const T zr = Real<T>::sq(rem);
+  const int k0 = (int)fmax(T(0), floor((cz - zr - oz) * ih));
+  const int k1 = (int)fmin(T(kp.nz - 1), floor((cz + zr - oz) * ih));
+  if (k0 > k1) return;
+  const int cb = (i * kp.ny + j) * kp.nz;
+  b = __ldg(&kp.cell_start[cb + k0]);
+  len = __ldg(&kp.cell_start[cb + k1 + 1]) - b;
+}
+
+// The (i,j) column range of the sphere of radius Rr around c.
+template <typename T>
+__device__ __forceinline__ int column_range(const KParams &kp, T cx, T cy, T Rr, int &i0, int &j0, int &nj,
+                                            float &inv_nj) {
+  const T ih = T(kp.inv_h), ox = T(kp.ox), oy = T(kp.oy);
+  i0 = (int)fmax(T(0), floor((cx - Rr - ox) * ih));
+  const int i1 = (int)fmin(T(kp.nx - 1), floor((cx + Rr - ox) * ih));
+  j0 = (int)fmax(T(0), floor((cy - Rr - oy) * ih));
+  const int j1 = (int)fmin(T(kp.ny - 1), floor((cy + Rr - oy) * ih));
+  nj = j1 - j0 + 1;
+  inv_nj = 1.0f / (float)(nj > 0 ? nj : 1);
+  return (i1 >= i0 && nj > 0) ? (i1 - i0 + 1) * nj : 0;
+}
+
+// Block-wide exclusive scan of len; total receives the block sum.  Ends
+// after one __syncthreads; sm_wsum may be rewritten only after another.
+template <int NT>
+__device__ __forceinline__ int block_excl_scan(int len, int lane, int w, int *sm_wsum, int &total) {
+  constexpr int NW = NT / 32;
+  int incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) sm_wsum[w] = incl;
+  __syncthreads();
+  int wofs = 0;
+  total = 0;
+#pragma unroll
+  for (int k = 0; k < NW; k++) {
+    const int ws = sm_wsum[k];
+    wofs += k < w ? ws : 0;
+    total += ws;
+  }
+  return incl + wofs - len;
+}
+
+// Visit candidates list[0..m) (list == nullptr: atoms 0..m): thread tid
+// takes t, t+NT, ... two per iteration for instruction-level parallelism.
+template <typename T, int NT, int GAS, bool HASQ>
+__device__ __forceinline__ void visit_list(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
+                                           const bool (&act)[GasShape<GAS>::NS], const int *list, int m, int tid,
+                                           Acc<T, GasShape<GAS>::NS> &acc) {
+  int t = tid;
+  for (; t + NT < m; t += 2 * NT) {
+    const Atom<T> a1 = load_atom<T, GAS>(kp, list ? list[t] : t);
+    const Atom<T> a2 = load_atom<T, GAS>(kp, list ? list[t + NT] : t + NT);
+    visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
+    visit_atom<T, GAS, HASQ>(kp, p, act, a2, acc);
+  }
+  if (t < m) {
+    const Atom<T> a1 = load_atom<T, GAS>(kp, list ? list[t] : t);
+    visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
+  }
+}
+
+// Steps whose candidates do not fit the list: the runs of the reach sphere,
+// flattened chunk by chunk.  Kept out of line (large targets only) and given
+// copies of the probe, so the common step's code stays compact and its
+// registers never need an address.
+template <typename T, int GAS> struct ProbeSites {
+  T p[GasShape<GAS>::NS][3];
+  bool act[GasShape<GAS>::NS];
+};
+template <typename T, int NT, int GAS, bool HASQ>
+__device__ __noinline__ Acc<T, GasShape<GAS>::NS> chunked_visits(const KParams *__restrict__ kpg,
+                                                                 const ProbeSites<T, GAS> ps, T cx, T cy, T cz,
+                                                                 T R, int tid, int *sm_list, int *sm_wsum,
+                                                                 uint32_t *nvis_out) {
+  const KParams &kp = *kpg;
+  const int lane = tid & 31, w = tid >> 5;
+  Acc<T, GasShape<GAS>::NS> acc;
+  acc.zero();
+  uint32_t nvis = 0;
+  int i0, j0, nj;
+  float inv_nj;
+  const int ncol = column_range(kp, cx, cy, R, i0, j0, nj, inv_nj);
+  for (int base = 0; base < ncol; base += NT) {
+    int b, len, total;
+    column_run(kp, base + tid, ncol, i0, j0, nj, inv_nj, cx, cy, cz, R, b, len);
+    const int excl = block_excl_scan<NT>(len, lane, w, sm_wsum, total);
+    for (int cs = 0; cs < total; cs += LCAP) {
+      // this thread's run, as far as it falls into the chunk [cs, cs + LCAP)
+      const int lo = max(excl, cs), hi = min(excl + len, cs + LCAP);
+      for (int q = lo; q < hi; q++) sm_list[q - cs] = b + (q - excl);
+      __syncthreads();
+      visit_list<T, NT, GAS, HASQ>(kp, ps.p, ps.act, sm_list, min(LCAP, total - cs), tid, acc);
+      __syncthreads();  // the chunk is rewritten next
+    }
+    if (total == 0) __syncthreads();  // sm_wsum is rewritten next (block-uniform branch)
+    nvis += (uint32_t)total;
+  }
+  *nvis_out = nvis;
+  return acc;
+}
 
 // Block-cooperative site forces for the warp pass: all NT threads of a CTA
-// evaluate one probe configuration.  Columns are split over the threads and
-// their z-runs are flattened into a candidate list in shared memory (an
-// exclusive block scan of the run lengths gives every run its place; chunks
-// of LCAP entries), so each thread reads candidate t, t+NT, ... directly, two
-// per iteration for instruction-level parallelism.  The sums are reduced per
-// warp with a reduce-scatter butterfly and then across warps in shared memory
-// in a fixed order, so every thread ends with identical bits.
+// evaluate one probe configuration.
+//
+// Candidates: small targets, and probes whose reach sphere holds the whole
+// target, visit every atom.  Otherwise the CTA keeps a candidate list in
+// shared memory (a Verlet list): the z-runs of the columns meeting a sphere
+// LSKIN wider than the reach, flattened by an exclusive block scan of the
+// run lengths.  While the probe's centre stays within LSKIN of where the list
+// was built, the sphere of the current step lies inside the list's sphere, so
+// the list is reused as is; the per-site cutoff tests then pick exactly the
+// pairs the reference sums.  A list longer than LCAP is not kept: such steps
+// flatten the runs of the reach sphere chunk by chunk.
+//
+// The sums are reduced per warp with a reduce-scatter butterfly and then
+// across warps in shared memory in a fixed order, so every thread ends with
+// identical bits.  All threads call this with identical arguments.
 //   sm_list: LCAP ints; sm_wsum: NT/32 ints; sm_red: (NT/32 + 1) * RedShape<GAS>::P values
+//   list_n, list_c: the CTA's list state (list_n < 0: no valid list)
 template <typename T, int NT, int GAS, bool HASQ>
 __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
                                                   const bool (&act)[GasShape<GAS>::NS], const T (&cen)[3],
                                                   T off, T (&f)[GasShape<GAS>::NS][3],
                                                   T (&U)[GasShape<GAS>::NS], uint32_t &visits, int tid,
-                                                  int *sm_list, int *sm_wsum, T *sm_red) {
+                                                  int *sm_list, int *sm_wsum, T *sm_red, int &list_n,
+                                                  T (&list_c)[3], const KParams *__restrict__ kpg) {
   constexpr int NS = GasShape<GAS>::NS;
   constexpr int NW = NT / 32;
   constexpr int NV = RedShape<GAS>::NV;
@@ -425,90 +563,51 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
     const T fx = fmax(cx - T(kp.bb_lo[0]), T(kp.bb_hi[0]) - cx);
     const T fy = fmax(cy - T(kp.bb_lo[1]), T(kp.bb_hi[1]) - cy);
     const T fz = fmax(cz - T(kp.bb_lo[2]), T(kp.bb_hi[2]) - cz);
-    if (fx * fx + fy * fy + fz * fz <= R * R) {
-      // the whole target inside the reach sphere: every atom is a candidate
-      int t = tid;
-      for (; t + NT < kp.natoms; t += 2 * NT) {
-        const Atom<T> a1 = load_atom<T, GAS>(kp, t);
-        const Atom<T> a2 = load_atom<T, GAS>(kp, t + NT);
-        visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
-        visit_atom<T, GAS, HASQ>(kp, p, act, a2, acc);
-      }
-      if (t < kp.natoms) {
-        const Atom<T> a1 = load_atom<T, GAS>(kp, t);
-        visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
-      }
-      nvis += (uint32_t)kp.natoms;
+    const int *lst = nullptr;  // candidates: atoms 0..m (nullptr) or lst[0..m)
+    int m = 0;
+    if (kp.natoms <= 2 * NT || fx * fx + fy * fy + fz * fz <= R * R) {
+      // the whole target inside the reach sphere, or a target of at most two
+      // atoms per thread: every atom is a candidate (the cutoff tests are exact)
+      m = kp.natoms;
     } else if (ex * ex + ey * ey + ez * ez <= R * R) {
-      const T ih = T(kp.inv_h), h = T(kp.h), ox = T(kp.ox), oy = T(kp.oy), oz = T(kp.oz);
-      const int i0 = (int)fmax(T(0), floor((cx - R - ox) * ih));
-      const int i1 = (int)fmin(T(kp.nx - 1), floor((cx + R - ox) * ih));
-      const int j0 = (int)fmax(T(0), floor((cy - R - oy) * ih));
-      const int j1 = (int)fmin(T(kp.ny - 1), floor((cy + R - oy) * ih));
-      const int nj = j1 - j0 + 1;
-      const int ncol = (i1 >= i0 && nj > 0) ? (i1 - i0 + 1) * nj : 0;
-      const float inv_nj = 1.0f / (float)(nj > 0 ? nj : 1);
-      for (int base = 0; base < ncol; base += NT) {
-        const int cidx = base + tid;
-        int b = 0, len = 0;
-        if (cidx < ncol) {
-          const int di = (int)(((float)cidx + 0.5f) * inv_nj);
-          const int i = i0 + di, j = j0 + (cidx - di * nj);
-          const T xlo = ox + T(i) * h, ylo = oy + T(j) * h;
-          const T dxc = fmax(fmax(xlo - cx, cx - (xlo + h)), T(0));
-          const T dyc = fmax(fmax(ylo - cy, cy - (ylo + h)), T(0));
-          const T rem = R * R - dxc * dxc - dyc * dyc;
-          if (rem >= T(0)) {
-            const T zr = Real<T>::sq(rem);
-            const int k0 = (int)fmax(T(0), floor((cz - zr - oz) * ih));
-            const int k1 = (int)fmin(T(kp.nz - 1), floor((cz + zr - oz) * ih));
-            if (k0 <= k1) {
-              const int cb = (i * kp.ny + j) * kp.nz;
-              b = __ldg(&kp.cell_start[cb + k0]);
-              len = __ldg(&kp.cell_start[cb + k1 + 1]) - b;
-            }
-          }
+      const T dcx = cx - list_c[0], dcy = cy - list_c[1], dcz = cz - list_c[2];
+      if (list_n < 0 || dcx * dcx + dcy * dcy + dcz * dcz > T(LSKIN) * T(LSKIN)) {
+        // rebuild the list for the sphere of radius R + LSKIN around the centre
+        const T RL = R + T(LSKIN);
+        int i0, j0, nj;
+        float inv_nj;
+        const int ncol = column_range(kp, cx, cy, RL, i0, j0, nj, inv_nj);
+        int filled = 0;  // block-uniform
+        for (int base = 0; base < ncol; base += NT) {
+          int b, len, total;
+          column_run(kp, base + tid, ncol, i0, j0, nj, inv_nj, cx, cy, cz, RL, b, len);
+          const int excl = block_excl_scan<NT>(len, lane, w, sm_wsum, total);
+          if (filled + total <= LCAP)
+            for (int q = 0; q < len; q++) sm_list[filled + excl + q] = b + q;
+          filled += total;
+          __syncthreads();  // the runs are in place; sm_wsum may be rewritten
         }
-        // block-wide exclusive scan of the run lengths
-        int incl = len;
+        list_n = filled <= LCAP ? filled : -1;
+        list_c[0] = cx; list_c[1] = cy; list_c[2] = cz;
+      }
+      if (list_n >= 0) {
+        lst = sm_list;
+        m = list_n;
+      } else {
+        ProbeSites<T, GAS> ps;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int v = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += v;
-        }
-        if (lane == 31) sm_wsum[w] = incl;
-        __syncthreads();
-        int wofs = 0, total = 0;
+        for (int s = 0; s < NS; s++) {
+          ps.act[s] = act[s];
 #pragma unroll
-        for (int k = 0; k < NW; k++) {
-          const int ws = sm_wsum[k];
-          wofs += k < w ? ws : 0;
-          total += ws;
+          for (int k = 0; k < 3; k++) ps.p[s][k] = p[s][k];
         }
-        const int excl = incl + wofs - len;
-        for (int cs = 0; cs < total; cs += LCAP) {
-          // this thread's run, as far as it falls into the chunk [cs, cs + LCAP)
-          const int lo = max(excl, cs), hi = min(excl + len, cs + LCAP);
-          for (int q = lo; q < hi; q++) sm_list[q - cs] = b + (q - excl);
-          __syncthreads();
-          const int m = min(LCAP, total - cs);
-          int t = tid;
-          for (; t + NT < m; t += 2 * NT) {
-            const Atom<T> a1 = load_atom<T, GAS>(kp, sm_list[t]);
-            const Atom<T> a2 = load_atom<T, GAS>(kp, sm_list[t + NT]);
-            visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
-            visit_atom<T, GAS, HASQ>(kp, p, act, a2, acc);
-          }
-          if (t < m) {
-            const Atom<T> a1 = load_atom<T, GAS>(kp, sm_list[t]);
-            visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
-          }
-          __syncthreads();  // the list and sm_wsum are rewritten next
-        }
-        if (total == 0) __syncthreads();  // sm_wsum is rewritten next (block-uniform branch)
-        nvis += (uint32_t)total;
+        uint32_t nc = 0;
+        acc = chunked_visits<T, NT, GAS, HASQ>(kpg, ps, cx, cy, cz, R, tid, sm_list, sm_wsum, &nc);
+        nvis += nc;
       }
     }
+    visit_list<T, NT, GAS, HASQ>(kp, p, act, lst, m, tid, acc);
+    nvis += (uint32_t)m;
   }
   // reduce-scatter per warp, then the warps in a fixed order
   T v[P];
@@ -661,7 +760,15 @@ template <typename T> __device__ __forceinline__ T angle3(const T a[3], const T 
   } else {
     const float cx = a[1] * b[2] - a[2] * b[1], cy = a[2] * b[0] - a[0] * b[2],
                 cz = a[0] * b[1] - a[1] * b[0];
-    return atan2f(sqrtf(cx * cx + cy * cy + cz * cz), dot3(a, b));
+    const float sn = sqrtf(cx * cx + cy * cy + cz * cz), cs = dot3(a, b);
+    // one step turns the probe by a small angle: there atan(t), t = sn/cs <
+    // 1/8, is its Maclaurin series to t^9 (truncation below 1.2e-11, far
+    // under FP32 rounding); atan2f elsewhere
+    if (cs > 0.f && sn < 0.125f * cs) {
+      const float t = __fdividef(sn, cs), t2 = t * t;
+      return t * (1.f + t2 * (-1.f / 3.f + t2 * (1.f / 5.f + t2 * (-1.f / 7.f + t2 * (1.f / 9.f)))));
+    }
+    return atan2f(sn, cs);
   }
 }
 // 1 - cos(chi) between the initial and final centre-of-mass velocities.
@@ -1185,6 +1292,8 @@ __global__ void __launch_bounds__(NT) resume_kernel(KParams kp, const KParams *_
     __syncthreads();
     if (idx >= np) break;
     LaneState<T> L = reinterpret_cast<const LaneState<T> *>(kp.park)[idx];
+    int list_n = -1;  // this trajectory's candidate list (none yet)
+    T list_c[3] = {T(0), T(0), T(0)};
     for (unsigned it = 1;; it++) {
       if ((it & 1023u) == 0) {
         if (tid == 0) sm_idx = (global_ns() > kp.deadline_ns || *(volatile int *)kp.error) ? 1ull : 0ull;
@@ -1205,7 +1314,7 @@ __global__ void __launch_bounds__(NT) resume_kernel(KParams kp, const KParams *_
 #pragma unroll
         for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
         eval_forces_block<T, NT, GAS, HASQ>(kp, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
-                                              tid, sm_list, sm_wsum, sm_red);
+                                              tid, sm_list, sm_wsum, sm_red, list_n, list_c, kpg);
       } else {
 #pragma unroll
         for (int s = 0; s < NS; s++) fs[s][0] = fs[s][1] = fs[s][2] = Us[s] = T(0);
@@ -1234,6 +1343,7 @@ __global__ void __launch_bounds__(NT) resume_kernel(KParams kp, const KParams *_
       }
       load_init<T, GAS>(L, lane_setup<T, GAS>(kpg, L.j));
       L.mode = M_RESTART;
+      list_n = -1;
     }
     __syncthreads();
   }
