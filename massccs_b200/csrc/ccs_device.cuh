@@ -230,172 +230,6 @@ __device__ __forceinline__ bool ref_inside(const KParams &kp, T x, T y, T z) {
   return idx >= 0 && idx < (long long)kp.ref_nx * kp.ref_ny * kp.ref_nz;
 }
 
-// Site forces of one probe configuration.  All G lanes of the group call it
-// with identical arguments; each lane gets the identical result.
-//   p       site positions, act: sites that feel the target
-//   cen     centre of the sites, off: largest |p_s - cen|
-template <typename T, int G, int GAS, bool HASQ>
-__device__ __forceinline__ void eval_forces(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
-                                         const bool (&act)[GasShape<GAS>::NS], const T (&cen)[3],
-                                         T off, T (&f)[GasShape<GAS>::NS][3],
-                                         T (&U)[GasShape<GAS>::NS], uint32_t &visits, int g,
-                                         unsigned mask, int *sm_end, int *sm_del) {
-  constexpr int NS = GasShape<GAS>::NS;
-  Acc<T, NS> acc;
-  acc.zero();
-  bool any = false;
-#pragma unroll
-  for (int s = 0; s < NS; s++) any |= act[s];
-  uint32_t nvis = 0;
-  if (any) {
-    // candidate sphere around the centre; +1e-3 A so rounding never drops a pair
-    const T R = kp.allpairs ? T(INFINITY) : T(kp.reach) + off + T(1e-3);
-    const T cx = cen[0], cy = cen[1], cz = cen[2];
-    const T ex = fmax(fmax(T(kp.bb_lo[0]) - cx, cx - T(kp.bb_hi[0])), T(0));
-    const T ey = fmax(fmax(T(kp.bb_lo[1]) - cy, cy - T(kp.bb_hi[1])), T(0));
-    const T ez = fmax(fmax(T(kp.bb_lo[2]) - cz, cz - T(kp.bb_hi[2])), T(0));
-    // the whole target inside the reach sphere: every atom is a candidate
-    const T fx = fmax(cx - T(kp.bb_lo[0]), T(kp.bb_hi[0]) - cx);
-    const T fy = fmax(cy - T(kp.bb_lo[1]), T(kp.bb_hi[1]) - cy);
-    const T fz = fmax(cz - T(kp.bb_lo[2]), T(kp.bb_hi[2]) - cz);
-    if ((G > 1 && kp.natoms <= 2 * G) || fx * fx + fy * fy + fz * fz <= R * R) {
-      // the whole target inside the reach sphere, or a target of at most two
-      // atoms per lane of the group: every atom is a candidate
-      for (int ai = g; ai < kp.natoms; ai += G) {
-        const Atom<T> a = load_atom<T, GAS>(kp, ai);
-        visit_atom<T, GAS, HASQ>(kp, p, act, a, acc);
-      }
-      if (G == 1 || g == 0) nvis += (uint32_t)kp.natoms;
-    } else if (ex * ex + ey * ey + ez * ez <= R * R) {
-      const T ih = T(kp.inv_h), h = T(kp.h), ox = T(kp.ox), oy = T(kp.oy), oz = T(kp.oz);
-      const int i0 = (int)fmax(T(0), floor((cx - R - ox) * ih));
-      const int i1 = (int)fmin(T(kp.nx - 1), floor((cx + R - ox) * ih));
-      const int j0 = (int)fmax(T(0), floor((cy - R - oy) * ih));
-      const int j1 = (int)fmin(T(kp.ny - 1), floor((cy + R - oy) * ih));
-      const int nj = j1 - j0 + 1;
-      const int ncol = (i1 >= i0 && nj > 0) ? (i1 - i0 + 1) * nj : 0;
-      const float inv_nj = 1.0f / (float)(nj > 0 ? nj : 1);
-      for (int base = 0; base < ncol; base += G) {
-        const int cidx = base + g;
-        int b = 0, len = 0;
-        if (cidx < ncol) {
-          const int di = (int)(((float)cidx + 0.5f) * inv_nj);  // exact: cidx < 2^20
-          const int i = i0 + di, j = j0 + (cidx - di * nj);
-          const T xlo = ox + T(i) * h, ylo = oy + T(j) * h;
-          const T dxc = fmax(fmax(xlo - cx, cx - (xlo + h)), T(0));
-          const T dyc = fmax(fmax(ylo - cy, cy - (ylo + h)), T(0));
-          const T rem = R * R - dxc * dxc - dyc * dyc;
-          if (rem >= T(0)) {
-            const T zr = Real<T>::sq(rem);
-            const int k0 = (int)fmax(T(0), floor((cz - zr - oz) * ih));
-            const int k1 = (int)fmin(T(kp.nz - 1), floor((cz + zr - oz) * ih));
-            if (k0 <= k1) {
-              const int cb = (i * kp.ny + j) * kp.nz;
-              b = __ldg(&kp.cell_start[cb + k0]);
-              len = __ldg(&kp.cell_start[cb + k1 + 1]) - b;
-            }
-          }
-        }
-        if constexpr (G == 1) {
-          nvis += (uint32_t)len;
-          for (int ai = b; ai < b + len; ai++) {
-            const Atom<T> a = load_atom<T, GAS>(kp, ai);
-            visit_atom<T, GAS, HASQ>(kp, p, act, a, acc);
-          }
-        } else {
-          // flatten the G runs of this chunk: inclusive scan of run lengths
-          int incl = len;
-#pragma unroll
-          for (int o = 1; o < G; o <<= 1) {
-            const int v = __shfl_up_sync(mask, incl, o, G);
-            if (g >= o) incl += v;
-          }
-          const int total = __shfl_sync(mask, incl, G - 1, G);
-          if (total == 0) continue;
-          sm_end[g] = incl;
-          sm_del[g] = b - (incl - len);
-          __syncwarp(mask);
-          int r = 0, cur_end = sm_end[0], cur_del = sm_del[0];
-          for (int t = g; t < total; t += G) {
-            while (t >= cur_end) { ++r; cur_end = sm_end[r]; cur_del = sm_del[r]; }
-            const Atom<T> a = load_atom<T, GAS>(kp, t + cur_del);
-            visit_atom<T, GAS, HASQ>(kp, p, act, a, acc);
-          }
-          if (g == 0) nvis += (uint32_t)total;
-          __syncwarp(mask);
-        }
-      }
-    }
-  }
-  if constexpr (G > 1) {
-#pragma unroll
-    for (int s = 0; s < NS; s++) {
-      acc.U[s] = group_sum<G>(acc.U[s], mask);
-#pragma unroll
-      for (int k = 0; k < 3; k++) acc.f[s][k] = group_sum<G>(acc.f[s][k], mask);
-    }
-    if (HASQ && kp.dip_on) {
-#pragma unroll
-      for (int k = 0; k < 3; k++) acc.E[k] = group_sum<G>(acc.E[k], mask);
-#pragma unroll
-      for (int k = 0; k < 6; k++) acc.G[k] = group_sum<G>(acc.G[k], mask);
-    }
-  }
-#pragma unroll
-  for (int s = 0; s < NS; s++) {
-    f[s][0] = acc.f[s][0]; f[s][1] = acc.f[s][1]; f[s][2] = acc.f[s][2]; U[s] = acc.U[s];
-  }
-  if (HASQ && kp.dip_on) {
-    // Force.cpp:483-487: f += alpha (E . grad) E ; U -= alpha/2 |E|^2
-    constexpr int d = GasShape<GAS>::DIP;
-    const T al = T(kp.alpha);
-    const T *E = acc.E, *Gr = acc.G;
-    f[d][0] += al * (E[0] * Gr[0] + E[1] * Gr[3] + E[2] * Gr[4]);
-    f[d][1] += al * (E[0] * Gr[3] + E[1] * Gr[1] + E[2] * Gr[5]);
-    f[d][2] += al * (E[0] * Gr[4] + E[1] * Gr[5] + E[2] * Gr[2]);
-    U[d] -= T(0.5) * al * (E[0] * E[0] + E[1] * E[1] + E[2] * E[2]);
-  }
-#pragma unroll
-  for (int s = 0; s < NS; s++)
-    if (!act[s]) { f[s][0] = f[s][1] = f[s][2] = U[s] = T(0); }
-  visits += nvis;
-}
-
-// Sum of P values over the 32 lanes of a warp, scattered: a reduce-scatter
-// butterfly in which each exchange sends half of the values still held, so
-// the warp spends 2P - 1 shuffles (not 5P).  Afterwards lane l holds in v[0]
-// the warp sum of value index (l >> (5 - log2 P)); lanes that share an index
-// hold identical bits (each pairwise sum is commutative).
-template <int O, int C, int P, typename T> __device__ __forceinline__ void rs_level(T (&v)[P], int lane) {
-  if constexpr (C == 1) {
-    v[0] += __shfl_xor_sync(0xffffffffu, v[0], O);
-  } else {
-    constexpr int H = C / 2;
-    const bool up = (lane & O) != 0;
-#pragma unroll
-    for (int i = 0; i < H; i++) {
-      const T send = up ? v[i] : v[i + H];
-      const T keep = up ? v[i + H] : v[i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, O);
-    }
-  }
-  if constexpr (O > 1) rs_level<O / 2, (C == 1 ? 1 : C / 2), P>(v, lane);
-}
-template <int P, typename T> __device__ __forceinline__ void warp_reduce_scatter(T (&v)[P], int lane) {
-  static_assert(P >= 1 && P <= 32 && (P & (P - 1)) == 0, "P must be a power of two <= 32");
-  rs_level<16, P, P>(v, lane);
-}
-template <int P> constexpr int log2_of() { return P <= 1 ? 0 : 1 + log2_of<P / 2>(); }
-
-// values reduced per force evaluation: per site f (3) and U, then the field
-// (3) and its gradient (6) at the dipole site; padded to a power of two
-template <int GAS> struct RedShape {
-  static constexpr int NV = 4 * GasShape<GAS>::NS + 9;
-  static constexpr int P = NV <= 16 ? 16 : 32;
-};
-constexpr int LCAP = 2048;  // candidate-list entries kept in shared memory per CTA
-constexpr float LSKIN = 1.0f;  // A: the list's margin; reused while the probe moves less
-
 // Column (i,j) number cidx of the ncol columns meeting the sphere of radius Rr
 // around c: its z-run of atoms [b, b + len) clipped to the sphere.
 template <typename T>
@@ -434,6 +268,196 @@ __device__ __forceinline__ int column_range(const KParams &kp, T cx, T cy, T Rr,
   inv_nj = 1.0f / (float)(nj > 0 ? nj : 1);
   return (i1 >= i0 && nj > 0) ? (i1 - i0 + 1) * nj : 0;
 }
+
+// Raw sums of one force evaluation, in row order: per site f (3) and U, then
+// the field (3) and its gradient (xx yy zz xy xz yz) at the dipole site.
+template <typename T, int NS> __device__ __forceinline__ T acc_value(const Acc<T, NS> &acc, int k) {
+  return k < 4 * NS ? (k % 4 == 3 ? acc.U[k / 4] : acc.f[k / 4][k % 4])
+                    : (k < 4 * NS + 3 ? acc.E[k - 4 * NS] : acc.G[k - 4 * NS - 3]);
+}
+
+// Site forces and energies from a row of raw sums: the induced-dipole force
+// alpha (E . grad) E and energy -alpha/2 |E|^2 (Force.cpp:483-487) at the
+// dipole site; sites outside the reference grid feel nothing.
+template <typename T, int GAS, bool HASQ>
+__device__ __forceinline__ void finish_row(const KParams &kp, const T *row, const bool (&act)[GasShape<GAS>::NS],
+                                           T (&f)[GasShape<GAS>::NS][3], T (&U)[GasShape<GAS>::NS]) {
+  constexpr int NS = GasShape<GAS>::NS;
+#pragma unroll
+  for (int s = 0; s < NS; s++) {
+    f[s][0] = row[4 * s]; f[s][1] = row[4 * s + 1]; f[s][2] = row[4 * s + 2]; U[s] = row[4 * s + 3];
+  }
+  if (HASQ && kp.dip_on) {
+    constexpr int d = GasShape<GAS>::DIP;
+    const T al = T(kp.alpha);
+    const T *E = row + 4 * NS, *Gr = row + 4 * NS + 3;
+    f[d][0] += al * (E[0] * Gr[0] + E[1] * Gr[3] + E[2] * Gr[4]);
+    f[d][1] += al * (E[0] * Gr[3] + E[1] * Gr[1] + E[2] * Gr[5]);
+    f[d][2] += al * (E[0] * Gr[4] + E[1] * Gr[5] + E[2] * Gr[2]);
+    U[d] -= T(0.5) * al * (E[0] * E[0] + E[1] * E[1] + E[2] * E[2]);
+  }
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+    if (!act[s]) { f[s][0] = f[s][1] = f[s][2] = U[s] = T(0); }
+}
+
+// Candidate visits of one probe configuration by a group of G lanes (G = 1:
+// one lane alone).  All lanes of the group call it with identical arguments;
+// each accumulates its share of the candidates into acc.
+//   p       site positions, act: sites that feel the target
+//   cen     centre of the sites, off: largest |p_s - cen|
+//   glist   the group's candidate buffer in shared memory, GCAP_PER_LANE * G ints
+constexpr int GCAP_PER_LANE = 8;
+template <typename T, int G, int GAS, bool HASQ>
+__device__ __forceinline__ void accumulate_group(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
+                                                 const bool (&act)[GasShape<GAS>::NS], const T (&cen)[3], T off,
+                                                 Acc<T, GasShape<GAS>::NS> &acc, uint32_t &visits, int g,
+                                                 unsigned mask, int *glist) {
+  constexpr int NS = GasShape<GAS>::NS;
+  constexpr int GCAP = GCAP_PER_LANE * G;
+  bool any = false;
+#pragma unroll
+  for (int s = 0; s < NS; s++) any |= act[s];
+  if (!any) return;
+  uint32_t nvis = 0;
+  // candidate sphere around the centre; +1e-3 A so rounding never drops a pair
+  const T R = kp.allpairs ? T(INFINITY) : T(kp.reach) + off + T(1e-3);
+  const T cx = cen[0], cy = cen[1], cz = cen[2];
+  const T ex = fmax(fmax(T(kp.bb_lo[0]) - cx, cx - T(kp.bb_hi[0])), T(0));
+  const T ey = fmax(fmax(T(kp.bb_lo[1]) - cy, cy - T(kp.bb_hi[1])), T(0));
+  const T ez = fmax(fmax(T(kp.bb_lo[2]) - cz, cz - T(kp.bb_hi[2])), T(0));
+  const T fx = fmax(cx - T(kp.bb_lo[0]), T(kp.bb_hi[0]) - cx);
+  const T fy = fmax(cy - T(kp.bb_lo[1]), T(kp.bb_hi[1]) - cy);
+  const T fz = fmax(cz - T(kp.bb_lo[2]), T(kp.bb_hi[2]) - cz);
+  if ((G > 1 && kp.natoms <= 2 * G) || fx * fx + fy * fy + fz * fz <= R * R) {
+    // the whole target inside the reach sphere, or a target of at most two
+    // atoms per lane of the group: every atom is a candidate
+    for (int ai = g; ai < kp.natoms; ai += G) {
+      const Atom<T> a = load_atom<T, GAS>(kp, ai);
+      visit_atom<T, GAS, HASQ>(kp, p, act, a, acc);
+    }
+    if (G == 1 || g == 0) nvis += (uint32_t)kp.natoms;
+  } else if (ex * ex + ey * ey + ez * ez <= R * R) {
+    int i0, j0, nj;
+    float inv_nj;
+    const int ncol = column_range(kp, cx, cy, R, i0, j0, nj, inv_nj);
+    for (int base = 0; base < ncol; base += G) {
+      int b, len;
+      column_run(kp, base + g, ncol, i0, j0, nj, inv_nj, cx, cy, cz, R, b, len);
+      if constexpr (G == 1) {
+        nvis += (uint32_t)len;
+        for (int ai = b; ai < b + len; ai++) {
+          const Atom<T> a = load_atom<T, GAS>(kp, ai);
+          visit_atom<T, GAS, HASQ>(kp, p, act, a, acc);
+        }
+      } else {
+        // flatten the G runs of this chunk into the group's list: exclusive scan of run lengths
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < G; o <<= 1) {
+          const int v = __shfl_up_sync(mask, incl, o, G);
+          if (g >= o) incl += v;
+        }
+        const int total = __shfl_sync(mask, incl, G - 1, G);
+        const int excl = incl - len;
+        for (int cs = 0; cs < total; cs += GCAP) {
+          const int lo = max(excl, cs), hi = min(excl + len, cs + GCAP);
+          for (int q = lo; q < hi; q++) glist[q - cs] = b + (q - excl);
+          __syncwarp(mask);
+          const int m = min(GCAP, total - cs);
+          for (int t = g; t < m; t += G) {
+            const Atom<T> a = load_atom<T, GAS>(kp, glist[t]);
+            visit_atom<T, GAS, HASQ>(kp, p, act, a, acc);
+          }
+          __syncwarp(mask);  // the list is rewritten next
+        }
+        if (g == 0) nvis += (uint32_t)total;
+      }
+    }
+  }
+  visits += nvis;
+}
+
+// Site forces of one probe configuration by a group of G lanes; every lane of
+// the group gets the identical result (xor-butterfly sums).  Used by the
+// force-evaluation entry point; the lane pass uses accumulate_group +
+// reduce_group_row instead.
+template <typename T, int G, int GAS, bool HASQ>
+__device__ __forceinline__ void eval_forces(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
+                                         const bool (&act)[GasShape<GAS>::NS], const T (&cen)[3],
+                                         T off, T (&f)[GasShape<GAS>::NS][3],
+                                         T (&U)[GasShape<GAS>::NS], uint32_t &visits, int g,
+                                         unsigned mask, int *glist) {
+  constexpr int NS = GasShape<GAS>::NS;
+  constexpr int NV = 4 * NS + 9;
+  Acc<T, NS> acc;
+  acc.zero();
+  accumulate_group<T, G, GAS, HASQ>(kp, p, act, cen, off, acc, visits, g, mask, glist);
+  T row[NV];
+#pragma unroll
+  for (int k = 0; k < NV; k++) row[k] = G > 1 ? group_sum<G>(acc_value(acc, k), mask) : acc_value(acc, k);
+  finish_row<T, GAS, HASQ>(kp, row, act, f, U);
+}
+
+// Sum of P values over the 32 lanes of a warp, scattered: a reduce-scatter
+// butterfly in which each exchange sends half of the values still held, so
+// the warp spends 2P - 1 shuffles (not 5P).  Afterwards lane l holds in v[0]
+// the warp sum of value index (l >> (5 - log2 P)); lanes that share an index
+// hold identical bits (each pairwise sum is commutative).
+template <int O, int C, int P, typename T> __device__ __forceinline__ void rs_level(T (&v)[P], int lane) {
+  if constexpr (C == 1) {
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], O);
+  } else {
+    constexpr int H = C / 2;
+    const bool up = (lane & O) != 0;
+#pragma unroll
+    for (int i = 0; i < H; i++) {
+      const T send = up ? v[i] : v[i + H];
+      const T keep = up ? v[i + H] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+    }
+  }
+  if constexpr (O > 1) rs_level<O / 2, (C == 1 ? 1 : C / 2), P>(v, lane);
+}
+template <int P, typename T> __device__ __forceinline__ void warp_reduce_scatter(T (&v)[P], int lane) {
+  static_assert(P >= 1 && P <= 32 && (P & (P - 1)) == 0, "P must be a power of two <= 32");
+  rs_level<16, P, P>(v, lane);
+}
+template <int P> constexpr int log2_of() { return P <= 1 ? 0 : 1 + log2_of<P / 2>(); }
+
+// values reduced per force evaluation: per site f (3) and U, then the field
+// (3) and its gradient (6) at the dipole site; padded to a power of two
+template <int GAS> struct RedShape {
+  static constexpr int NV = 4 * GasShape<GAS>::NS + 9;
+  static constexpr int P = NV <= 16 ? 16 : 32;
+};
+// Raw sums of a group's evaluation into row[0..NV) (shared memory).  A full
+// warp reduce-scatters (2P - 1 shuffles, each lane stores the value it ends
+// with); smaller groups sum every value by xor butterfly and lane 0 stores.
+template <typename T, int G, int GAS>
+__device__ __forceinline__ void reduce_group_row(const Acc<T, GasShape<GAS>::NS> &acc, int g, unsigned mask,
+                                                 T *row) {
+  constexpr int NS = GasShape<GAS>::NS;
+  constexpr int NV = RedShape<GAS>::NV;
+  if constexpr (G == 32) {
+    constexpr int P = RedShape<GAS>::P;
+    T v[P];
+#pragma unroll
+    for (int k = 0; k < P; k++) v[k] = k < NV ? acc_value(acc, k) : T(0);
+    warp_reduce_scatter<P>(v, g);
+    constexpr int SH = 5 - log2_of<P>();
+    if ((g & ((1 << SH) - 1)) == 0 && (g >> SH) < NV) row[g >> SH] = v[0];
+  } else {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      const T x = G > 1 ? group_sum<G>(acc_value(acc, k), mask) : acc_value(acc, k);
+      if (g == 0) row[k] = x;
+    }
+  }
+}
+
+constexpr int LCAP = 2048;  // candidate-list entries kept in shared memory per CTA
+constexpr float LSKIN = 1.0f;  // A: the list's margin; reused while the probe moves less
 
 // Block-wide exclusive scan of len; total receives the block sum.  Ends
 // after one __syncthreads; sm_wsum may be rewritten only after another.
@@ -1103,11 +1127,12 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
   constexpr int NS = S::NS;
   constexpr int NSUB = 32 / G;
   constexpr unsigned FULL = 0xffffffffu;
+  constexpr int NV = RedShape<GAS>::NV;
   __shared__ T sm_pos[BLOCK][NS][3];
-  __shared__ T sm_res[BLOCK][NS][4];
+  __shared__ T sm_row[BLOCK][NV];
   __shared__ uint32_t sm_vis[BLOCK];
   __shared__ unsigned sm_act[BLOCK];
-  __shared__ int sm_end[BLOCK], sm_del[BLOCK];
+  __shared__ int sm_glist[BLOCK * GCAP_PER_LANE];
   __shared__ unsigned long long blk[8];
   if (threadIdx.x < 8) blk[threadIdx.x] = 0ull;
   __syncthreads();
@@ -1172,7 +1197,7 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
 #pragma unroll
           for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
           eval_forces<T, 1, GAS, HASQ>(kp, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis, 0,
-                                       1u << lane, nullptr, nullptr);
+                                       1u << lane, nullptr);
         } else {
 #pragma unroll
           for (int s = 0; s < NS; s++)
@@ -1188,7 +1213,7 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
       const int nn = __popc(bal);
       for (int idx = sub; idx < nn; idx += NSUB) {
         const int t = wbase + nth_set_bit(bal, idx);
-        T P[NS][3], ff[NS][3], UU[NS];
+        T P[NS][3];
         bool act[NS];
         const unsigned ab = sm_act[t];
 #pragma unroll
@@ -1198,24 +1223,19 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
           for (int k = 0; k < 3; k++) P[s][k] = sm_pos[t][s][k];
         }
         uint32_t nv = 0;
-        eval_forces<T, G, GAS, HASQ>(kp, P, act, P[S::cs], site_offset<T, GAS>(P), ff, UU, nv, g, gmask,
-                                     sm_end + wbase + sub * G, sm_del + wbase + sub * G);
-        if (g == 0) {
-#pragma unroll
-          for (int s = 0; s < NS; s++) {
-            sm_res[t][s][0] = ff[s][0]; sm_res[t][s][1] = ff[s][1];
-            sm_res[t][s][2] = ff[s][2]; sm_res[t][s][3] = UU[s];
-          }
-          sm_vis[t] = nv;
-        }
+        Acc<T, NS> acc;
+        acc.zero();
+        accumulate_group<T, G, GAS, HASQ>(kp, P, act, P[S::cs], site_offset<T, GAS>(P), acc, nv, g, gmask,
+                                          sm_glist + (wbase + sub * G) * GCAP_PER_LANE);
+        reduce_group_row<T, G, GAS>(acc, g, gmask, sm_row[t]);
+        if (g == 0) sm_vis[t] = nv;
       }
       __syncwarp();
-      if (near) {
+      if (near) {  // the probe's own lane finishes its forces from the raw sums
+        bool act[NS];
 #pragma unroll
-        for (int s = 0; s < NS; s++) {
-          fs[s][0] = sm_res[threadIdx.x][s][0]; fs[s][1] = sm_res[threadIdx.x][s][1];
-          fs[s][2] = sm_res[threadIdx.x][s][2]; Us[s] = sm_res[threadIdx.x][s][3];
-        }
+        for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
+        finish_row<T, GAS, HASQ>(kp, sm_row[threadIdx.x], act, fs, Us);
         L.nvis += sm_vis[threadIdx.x];
       }
     }
@@ -1357,7 +1377,7 @@ __global__ void __launch_bounds__(BLOCK)
     force_points_kernel(KParams kp, int site, size_t npts, const double *pts, double *f, double *U,
                         uint32_t *vis) {
   constexpr int NS = GasShape<GAS>::NS;
-  __shared__ int sm_end[BLOCK], sm_del[BLOCK];
+  __shared__ int sm_glist[BLOCK * GCAP_PER_LANE];
   const int lane = threadIdx.x & 31;
   const int g = lane & (G - 1);
   const unsigned mask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lane & ~(G - 1)));
@@ -1373,7 +1393,7 @@ __global__ void __launch_bounds__(BLOCK)
     }
     uint32_t v = 0;
     eval_forces<T, G, GAS, HASQ>(kp, p, act, cen, T(0), ff, UU, v, g, mask,
-                                 sm_end + (threadIdx.x & ~(G - 1)), sm_del + (threadIdx.x & ~(G - 1)));
+                                 sm_glist + (threadIdx.x & ~(G - 1)) * GCAP_PER_LANE);
     if (g == 0) {
       for (int k = 0; k < 3; k++) f[3 * i + k] = (double)ff[site][k];
       U[i] = (double)UU[site];
