@@ -92,7 +92,7 @@ typedef struct {
   uint32_t max_steps_per_try; /* 0 = 2,000,000 */
   double watchdog_s;        /* kernel wall-time budget, 0 = 600 s */
   int32_t schedule;         /* 0 = index order, 1 = longest expected trajectories first */
-  uint32_t park_steps;      /* steps after which a trajectory moves to the warp pass; 0 = 4096 */
+  uint32_t park_steps;      /* steps after which a trajectory moves to the warp pass; 0 = 2048 */
   int32_t resume_block;     /* threads per trajectory in the warp pass: 32, 64 or 128; 0 = 64 */
 } ccs_params;
 

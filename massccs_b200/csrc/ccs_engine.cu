@@ -388,7 +388,7 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   }
   k.park = c->d_park;
   k.park_cap = cap;
-  k.park_steps = c->p.park_steps ? c->p.park_steps : 4096u;
+  k.park_steps = c->p.park_steps ? c->p.park_steps : 2048u;
   k.park_count = c->d_work + 9;
   k.park_next = c->d_work + 10;
   // d_work: [0] work counter, [1..7] statistics, [8] clock scratch, [9] parked, [10] resumed
@@ -1001,7 +1001,7 @@ extern "C" int ccs_run_device_noalloc(ccs_ctx *c, size_t n, const double *d_rnd,
   k.error = error;
   k.park = park;
   k.park_cap = std::min<size_t>(n, NOALLOC_PARK_CAP);
-  k.park_steps = c->p.park_steps ? c->p.park_steps : 4096u;
+  k.park_steps = c->p.park_steps ? c->p.park_steps : 2048u;
   k.park_count = work + 9;
   k.park_next = work + 10;
   // everything that must start at zero: counters, statistics, park counters, error flag
