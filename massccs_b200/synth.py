@@ -124,7 +124,7 @@ def write_xyz(path, sym, xyz, q, float32=False):
             f.write(f"{s} {x:.9g} {y:.9g} {z:.9g} {c:.9g}\n")
 
 
-def write_input(d, target, gas, ft, nprobe, niter, seed=2104, ff=None, extra=None):
+def write_input(d, target, gas, ft, nprobe, niter, seed=2104, ff=None, extra=None, name="input.json"):
     kind = "mol" if gas in ("N2", "CO2") else "atom"
     fl = FLAGS[(kind, ft)]
     cfg = {"targetFileName": target, "numberProbe": int(nprobe), "nIter": int(niter), "seed": seed,
@@ -135,7 +135,7 @@ def write_input(d, target, gas, ft, nprobe, niter, seed=2104, ff=None, extra=Non
         cfg["force-field"] = ff
     if extra:
         cfg.update(extra)
-    p = os.path.join(d, "input.json")
+    p = os.path.join(d, name)
     with open(p, "w") as f:
         json.dump(cfg, f, indent=1)
     return p
