@@ -145,6 +145,21 @@ int ccs_set_params(ccs_ctx *ctx, const ccs_params *p);
 int ccs_run(ccs_ctx *ctx, size_t ntraj, const double *const rnd[9], int8_t *status,
             double *one_minus_cos, uint32_t *steps, uint32_t *visits, ccs_stats *stats);
 
+/* Many ions in one launch of each pass (batched ions of uneven size).  No
+ * counterpart in the reference, which runs one ion per process: a caller with
+ * several ions replaces their separate System::System runs
+ * (src/System.cpp:146-321) by one call.  ions[i] is a context set up for ion
+ * i (ccs_set_params + ccs_set_target), all on one device, with one precision,
+ * and all atomic or all molecular gases; ntraj[i] its trajectory count.
+ * rnd[k] holds row k of every ion's pre-draw back to back (ion 0 first), and
+ * status / one_minus_cos / steps / visits are laid out the same way.  The
+ * first context's stream, scratch and statistics carry the run; lanes per
+ * force evaluation are its lanes_per_traj (8, 16 or 32), else autotuned on a
+ * sub-batch of every ion's first trajectories.  Synchronous. */
+int ccs_run_batch(ccs_ctx *const *ions, size_t nions, const size_t *ntraj, const double *const rnd[9],
+                  int8_t *status, double *one_minus_cos, uint32_t *steps, uint32_t *visits,
+                  ccs_stats *stats);
+
 /* Same on device buffers, asynchronous on `stream` (a cudaStream_t, NULL =
  * the context's stream).  d_rnd holds 9 rows of `stride` doubles.  Statistics
  * are accumulated on the device and read back by ccs_sync_stats. */

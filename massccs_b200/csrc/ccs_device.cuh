@@ -86,6 +86,12 @@ struct KParams {
   unsigned long long *park_next;    // next parked trajectory to resume
   unsigned long long park_cap;
   uint32_t park_steps;
+  // batched ions: per-ion parameters (their rnd/status/omc/steps/visits point
+  // at the ion's first trajectory) and the global index of each ion's first
+  // trajectory (nions + 1 entries); unused by single-ion runs
+  const struct KParams *ions;
+  const unsigned long long *ion_start;
+  int nions;
   int *error;                 // 1 = watchdog
 };
 
@@ -856,6 +862,7 @@ template <typename T> struct LaneState {
   T U, rold[3], dtheta, dt, Ei;
   uint32_t stepcount, nsteps, nvis;
   int tries, maxTries, mode;
+  uint32_t ion;  // batched runs: the trajectory's ion (j is its index within that ion)
   unsigned long long j;
 };
 
@@ -1121,7 +1128,18 @@ __device__ __forceinline__ void write_result(const KParams &kp, const LaneState<
   atomicAdd(&blk[5], (unsigned long long)L.nvis);
 }
 
-template <typename T, int G, int GAS, bool HASQ>
+// Parameters of the ion that trajectory state L belongs to: the launch's own
+// (constant bank) for single-ion runs, the ion's entry of kp.ions for batches.
+template <bool BATCH>
+__device__ __forceinline__ const KParams &ion_params(const KParams &kp, uint32_t ion) {
+  if constexpr (BATCH) return kp.ions[ion]; else return kp;
+}
+template <bool BATCH>
+__device__ __forceinline__ const KParams *ion_params_ptr(const KParams &kp, const KParams *kpg, uint32_t ion) {
+  if constexpr (BATCH) return kp.ions + ion; else return kpg;
+}
+
+template <typename T, int G, int GAS, bool HASQ, bool BATCH>
 __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParams *__restrict__ kpg) {
   using S = Sites<GAS>;
   constexpr int NS = S::NS;
@@ -1132,6 +1150,7 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
   __shared__ T sm_row[BLOCK][NV];
   __shared__ uint32_t sm_vis[BLOCK];
   __shared__ unsigned sm_act[BLOCK];
+  __shared__ uint32_t sm_ion[BATCH ? BLOCK : 1];
   __shared__ int sm_glist[BLOCK * GCAP_PER_LANE];
   __shared__ unsigned long long blk[8];
   if (threadIdx.x < 8) blk[threadIdx.x] = 0ull;
@@ -1145,22 +1164,35 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
 
   LaneState<T> L;
   L.mode = M_IDLE;
+  L.ion = 0;
 
   // take trajectories until one hits the ellipsoid (misses are written as free)
   auto grab = [&]() {
     for (;;) {
       const unsigned long long jj = atomicAdd(kp.work, 1ull);
       if (jj >= kp.ntraj || *(volatile int *)kp.error) { L.mode = M_IDLE; return; }
-      L.j = kp.order ? (unsigned long long)__ldg(&kp.order[jj]) : jj;
+      if constexpr (BATCH) {  // the ion holding global trajectory jj (bisection of the ion starts)
+        int lo = 0, hi = kp.nions;
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (__ldg(&kp.ion_start[mid]) <= jj) lo = mid; else hi = mid;
+        }
+        L.ion = (uint32_t)lo;
+        L.j = jj - __ldg(&kp.ion_start[lo]);
+      } else {
+        L.ion = 0;
+        L.j = kp.order ? (unsigned long long)__ldg(&kp.order[jj]) : jj;
+      }
+      const KParams &K = ion_params<BATCH>(kp, L.ion);
       L.nsteps = 0;
       L.nvis = 0;
-      const InitState<T> I = lane_setup<T, GAS>(kpg, L.j);
-      if (!I.hit) { write_result(kp, L, 0, 0.0, blk); continue; }
+      const InitState<T> I = lane_setup<T, GAS>(ion_params_ptr<BATCH>(kp, kpg, L.ion), L.j);
+      if (!I.hit) { write_result(K, L, 0, 0.0, blk); continue; }
       load_init<T, GAS>(L, I);
       L.Ei = I.ek;  // completed with the initial potential energy by the first force phase
       L.tries = 0;
       L.maxTries = 8;
-      L.dt = T(kp.dt);
+      L.dt = T(K.dt);
       L.mode = M_INIT;
       return;
     }
@@ -1175,13 +1207,14 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
       e = __shfl_sync(FULL, e, 0);
       if (e) {
         if (lane == 0) atomicExch(kp.error, 1);
-        if (L.mode != M_IDLE) write_result(kp, L, 3, 0.0, blk);
+        if (L.mode != M_IDLE) write_result(ion_params<BATCH>(kp, L.ion), L, 3, 0.0, blk);
         L.mode = M_IDLE;
       }
     }
     if (__all_sync(FULL, L.mode == M_IDLE)) break;
+    const KParams &K = ion_params<BATCH>(kp, L.ion);  // this lane's ion
 
-    if (L.mode == M_STEP) first_half<T, GAS>(kp, L);
+    if (L.mode == M_STEP) first_half<T, GAS>(K, L);
 
     // ---- force phase
     bool near = false;
@@ -1190,13 +1223,13 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
     if (L.mode != M_IDLE) {
       T p[NS][3];
       site_positions<T, GAS>(L, p);
-      near = probe_near<T, GAS>(kp, p, actbits);
+      near = probe_near<T, GAS>(K, p, actbits);
       if (near) {
         if constexpr (G == 1) {
           bool act[NS];
 #pragma unroll
           for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
-          eval_forces<T, 1, GAS, HASQ>(kp, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis, 0,
+          eval_forces<T, 1, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis, 0,
                                        1u << lane, nullptr);
         } else {
 #pragma unroll
@@ -1204,6 +1237,7 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
 #pragma unroll
             for (int k = 0; k < 3; k++) sm_pos[threadIdx.x][s][k] = p[s][k];
           sm_act[threadIdx.x] = actbits;
+          if constexpr (BATCH) sm_ion[threadIdx.x] = L.ion;
         }
       }
     }
@@ -1225,7 +1259,8 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
         uint32_t nv = 0;
         Acc<T, NS> acc;
         acc.zero();
-        accumulate_group<T, G, GAS, HASQ>(kp, P, act, P[S::cs], site_offset<T, GAS>(P), acc, nv, g, gmask,
+        const KParams &Kt = ion_params<BATCH>(kp, BATCH ? sm_ion[t] : 0u);  // the probe's ion
+        accumulate_group<T, G, GAS, HASQ>(Kt, P, act, P[S::cs], site_offset<T, GAS>(P), acc, nv, g, gmask,
                                           sm_glist + (wbase + sub * G) * GCAP_PER_LANE);
         reduce_group_row<T, G, GAS>(acc, g, gmask, sm_row[t]);
         if (g == 0) sm_vis[t] = nv;
@@ -1235,7 +1270,7 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
         bool act[NS];
 #pragma unroll
         for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
-        finish_row<T, GAS, HASQ>(kp, sm_row[threadIdx.x], act, fs, Us);
+        finish_row<T, GAS, HASQ>(K, sm_row[threadIdx.x], act, fs, Us);
         L.nvis += sm_vis[threadIdx.x];
       }
     }
@@ -1244,7 +1279,7 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
 #pragma unroll
       for (int s = 0; s < NS; s++) fs[s][0] = fs[s][1] = fs[s][2] = Us[s] = T(0);
     }
-    absorb_forces<T, GAS>(kp, fs, Us, L);
+    absorb_forces<T, GAS>(K, fs, Us, L);
 
     // ---- second half, exit tests, retries, parking
     if (L.mode == M_INIT) {
@@ -1254,23 +1289,23 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
       L.mode = M_STEP;
     } else {
       T vc[3];
-      const int r = second_half<T, GAS>(kp, L, vc);
+      const int r = second_half<T, GAS>(K, L, vc);
       if (r == S_SCATTER) {
-        write_result(kp, L, 1, lane_chi<T, GAS>(kpg, L.j, vc[0], vc[1], vc[2]), blk);
+        write_result(K, L, 1, lane_chi<T, GAS>(ion_params_ptr<BATCH>(kp, kpg, L.ion), L.j, vc[0], vc[1], vc[2]), blk);
         grab();
       } else if (r == S_CAPPED) {
-        write_result(kp, L, 3, 0.0, blk);
+        write_result(K, L, 3, 0.0, blk);
         grab();
       } else if (r != S_CONTINUE) {
         // a failed try: smaller time step and a fresh start (System.cpp:453-458, 468-473)
         L.tries++;
         if (r == S_RETRY_ENERGY) L.maxTries++;
-        L.dt = T(kp.dt / (L.tries + 1));
+        L.dt = T(K.dt / (L.tries + 1));
         if (!(L.tries < L.maxTries && L.maxTries < 10)) {
-          write_result(kp, L, 2, 0.0, blk);
+          write_result(K, L, 2, 0.0, blk);
           grab();
         } else {
-          load_init<T, GAS>(L, lane_setup<T, GAS>(kpg, L.j));
+          load_init<T, GAS>(L, lane_setup<T, GAS>(ion_params_ptr<BATCH>(kp, kpg, L.ion), L.j));
           L.mode = M_RESTART;
         }
       } else if (kp.park && L.nsteps >= kp.park_steps) {
@@ -1292,7 +1327,7 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
 // the same state; the force phase is block-cooperative).
 constexpr int RBLOCK = 64;  // default threads per trajectory in the warp pass
 
-template <typename T, int GAS, bool HASQ, int NT>
+template <typename T, int GAS, bool HASQ, int NT, bool BATCH>
 __global__ void __launch_bounds__(NT) resume_kernel(KParams kp, const KParams *__restrict__ kpg) {
   using S = Sites<GAS>;
   constexpr int NS = S::NS;
@@ -1312,6 +1347,8 @@ __global__ void __launch_bounds__(NT) resume_kernel(KParams kp, const KParams *_
     __syncthreads();
     if (idx >= np) break;
     LaneState<T> L = reinterpret_cast<const LaneState<T> *>(kp.park)[idx];
+    const KParams &K = ion_params<BATCH>(kp, L.ion);
+    const KParams *Kg = ion_params_ptr<BATCH>(kp, kpg, L.ion);
     int list_n = -1;  // this trajectory's candidate list (none yet)
     T list_c[3] = {T(0), T(0), T(0)};
     for (unsigned it = 1;; it++) {
@@ -1321,47 +1358,47 @@ __global__ void __launch_bounds__(NT) resume_kernel(KParams kp, const KParams *_
         const bool e = sm_idx != 0;
         __syncthreads();
         if (e) {
-          if (tid == 0) { atomicExch(kp.error, 1); write_result(kp, L, 3, 0.0, blk); }
+          if (tid == 0) { atomicExch(kp.error, 1); write_result(K, L, 3, 0.0, blk); }
           break;
         }
       }
-      if (L.mode == M_STEP) first_half<T, GAS>(kp, L);
+      if (L.mode == M_STEP) first_half<T, GAS>(K, L);
       T p[NS][3], fs[NS][3], Us[NS];
       site_positions<T, GAS>(L, p);
       unsigned actbits;
-      if (probe_near<T, GAS>(kp, p, actbits)) {
+      if (probe_near<T, GAS>(K, p, actbits)) {
         bool act[NS];
 #pragma unroll
         for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
-        eval_forces_block<T, NT, GAS, HASQ>(kp, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
-                                              tid, sm_list, sm_wsum, sm_red, list_n, list_c, kpg);
+        eval_forces_block<T, NT, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
+                                              tid, sm_list, sm_wsum, sm_red, list_n, list_c, Kg);
       } else {
 #pragma unroll
         for (int s = 0; s < NS; s++) fs[s][0] = fs[s][1] = fs[s][2] = Us[s] = T(0);
       }
-      absorb_forces<T, GAS>(kp, fs, Us, L);
+      absorb_forces<T, GAS>(K, fs, Us, L);
       if (L.mode == M_INIT) { L.Ei += L.U; L.mode = M_STEP; continue; }
       if (L.mode == M_RESTART) { L.mode = M_STEP; continue; }
       T vc[3];
-      const int r = second_half<T, GAS>(kp, L, vc);
+      const int r = second_half<T, GAS>(K, L, vc);
       if (r == S_CONTINUE) continue;
       if (r == S_SCATTER) {
-        const double omc = lane_chi<T, GAS>(kpg, L.j, vc[0], vc[1], vc[2]);
-        if (tid == 0) write_result(kp, L, 1, omc, blk);
+        const double omc = lane_chi<T, GAS>(Kg, L.j, vc[0], vc[1], vc[2]);
+        if (tid == 0) write_result(K, L, 1, omc, blk);
         break;
       }
       if (r == S_CAPPED) {
-        if (tid == 0) write_result(kp, L, 3, 0.0, blk);
+        if (tid == 0) write_result(K, L, 3, 0.0, blk);
         break;
       }
       L.tries++;
       if (r == S_RETRY_ENERGY) L.maxTries++;
-      L.dt = T(kp.dt / (L.tries + 1));
+      L.dt = T(K.dt / (L.tries + 1));
       if (!(L.tries < L.maxTries && L.maxTries < 10)) {
-        if (tid == 0) write_result(kp, L, 2, 0.0, blk);
+        if (tid == 0) write_result(K, L, 2, 0.0, blk);
         break;
       }
-      load_init<T, GAS>(L, lane_setup<T, GAS>(kpg, L.j));
+      load_init<T, GAS>(L, lane_setup<T, GAS>(Kg, L.j));
       L.mode = M_RESTART;
       list_n = -1;
     }

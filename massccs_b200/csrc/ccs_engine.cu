@@ -66,6 +66,10 @@ struct ccs_ctx {
   // device copy of the launch parameters (read by the non-inlined set-up code)
   KParams *d_kparams = nullptr;
   KParams h_kparams{};
+  // batched runs led by this context: the ions' parameters and first trajectories
+  KParams *d_bkp = nullptr;
+  unsigned long long *d_bstart = nullptr;
+  size_t bkp_cap = 0;
   // launch choice
   int tuned_G = 0, tuned_block = 0;
   ccs_stats last{};
@@ -154,12 +158,12 @@ void vel_table(double m_amu, double T, std::vector<double> &V, std::vector<doubl
 
 using KernelFn = void (*)(KParams, const KParams *);
 template <typename T, int GAS, bool HASQ> KernelFn resume_ptr(int nt) {
-  return nt == 32 ? resume_kernel<T, GAS, HASQ, 32> : nt == 64 ? resume_kernel<T, GAS, HASQ, 64>
-                                                               : resume_kernel<T, GAS, HASQ, 128>;
+  return nt == 32 ? resume_kernel<T, GAS, HASQ, 32, false>
+                  : nt == 64 ? resume_kernel<T, GAS, HASQ, 64, false> : resume_kernel<T, GAS, HASQ, 128, false>;
 }
 using ForceFn = void (*)(KParams, int, size_t, const double *, double *, double *, uint32_t *);
 
-template <typename T, int G, int GAS, bool HASQ> KernelFn traj_ptr() { return traj_kernel<T, G, GAS, HASQ>; }
+template <typename T, int G, int GAS, bool HASQ> KernelFn traj_ptr() { return traj_kernel<T, G, GAS, HASQ, false>; }
 template <typename T, int G, int GAS, bool HASQ> ForceFn force_ptr() {
   return force_points_kernel<T, G, GAS, HASQ>;
 }
@@ -466,6 +470,147 @@ int autotune(ccs_ctx *c, size_t n, size_t stride, int block) {
   return CCS_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Batched ions: one launch of each pass over the trajectories of many ions.
+// Every ion keeps its own context (parameters, target tables, cell grid); the
+// kernels pick the ion's parameters per trajectory from a device array.
+template <typename T, int G, int GAS, bool HASQ> KernelFn traj_batch_ptr() {
+  return traj_kernel<T, G, GAS, HASQ, true>;
+}
+template <typename T, int GAS, bool HASQ> KernelFn pick_traj_batch_g(int G) {
+  return G <= 8 ? traj_batch_ptr<T, 8, GAS, HASQ>()
+                : G == 16 ? traj_batch_ptr<T, 16, GAS, HASQ>() : traj_batch_ptr<T, 32, GAS, HASQ>();
+}
+template <typename T> KernelFn pick_traj_batch_t(int gas, bool hasq, int G) {
+  if (gas == GAS_ATOM) return hasq ? pick_traj_batch_g<T, GAS_ATOM, true>(G) : pick_traj_batch_g<T, GAS_ATOM, false>(G);
+  if (gas == GAS_N2) return hasq ? pick_traj_batch_g<T, GAS_N2, true>(G) : pick_traj_batch_g<T, GAS_N2, false>(G);
+  return hasq ? pick_traj_batch_g<T, GAS_CO2, true>(G) : pick_traj_batch_g<T, GAS_CO2, false>(G);
+}
+template <typename T> KernelFn pick_resume_batch_t(int gas, bool hasq) {
+  if (gas == GAS_ATOM)
+    return hasq ? resume_kernel<T, GAS_ATOM, true, RBLOCK, true> : resume_kernel<T, GAS_ATOM, false, RBLOCK, true>;
+  if (gas == GAS_N2)
+    return hasq ? resume_kernel<T, GAS_N2, true, RBLOCK, true> : resume_kernel<T, GAS_N2, false, RBLOCK, true>;
+  return hasq ? resume_kernel<T, GAS_CO2, true, RBLOCK, true> : resume_kernel<T, GAS_CO2, false, RBLOCK, true>;
+}
+int batch_lanes(int G) { return G <= 8 ? 8 : G <= 16 ? 16 : 32; }
+
+// Both passes over trajectories [0, m[i]) of every ion i, whose random rows
+// and outputs start at column off[i] of the lead context's buffers (row
+// stride `stride`).  Asynchronous on the lead's stream; events ev[5..7].
+int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const size_t *m, const size_t *off,
+                     size_t stride, bool want_steps, bool want_visits, int G) {
+  ccs_ctx *c = lead;  // error reports go to the lead context
+  cudaStream_t s = lead->stream;
+  std::vector<KParams> kv(nions);
+  std::vector<unsigned long long> st(nions + 1);
+  unsigned long long total = 0;
+  bool hasq = false;
+  for (size_t i = 0; i < nions; i++) {
+    const ccs_ctx *ci = ions[i];
+    KParams k = base_params(ci);
+    k.rnd = lead->d_rnd + off[i];
+    k.rnd_stride = stride;
+    k.ntraj = m[i];
+    k.status = lead->d_status + off[i];
+    k.omc = lead->d_omc + off[i];
+    k.steps = want_steps ? lead->d_steps + off[i] : nullptr;
+    k.visits = want_visits ? lead->d_visits + off[i] : nullptr;
+    k.order = nullptr;
+    kv[i] = k;
+    st[i] = total;
+    total += m[i];
+    hasq |= ci->coul_on || ci->dip_on;
+  }
+  st[nions] = total;
+  if (total == 0) return CCS_OK;
+  if (nions > lead->bkp_cap) {
+    dfree(lead->d_bkp); dfree(lead->d_bstart);
+    lead->bkp_cap = 0;
+    CK(cudaMalloc(&lead->d_bkp, nions * sizeof(KParams)));
+    CK(cudaMalloc(&lead->d_bstart, (nions + 1) * sizeof(unsigned long long)));
+    lead->bkp_cap = nions;
+  }
+  CK(cudaMemcpy(lead->d_bkp, kv.data(), nions * sizeof(KParams), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(lead->d_bstart, st.data(), (nions + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+  KParams k = base_params(lead);
+  k.ntraj = total;
+  k.ions = lead->d_bkp;
+  k.ion_start = lead->d_bstart;
+  k.nions = (int)nions;
+  unsigned long long now = 0;
+  int rc = device_now_ns(lead, now);
+  if (rc) return rc;
+  const double wd = lead->p.watchdog_s > 0 ? lead->p.watchdog_s : 600.0;
+  k.deadline_ns = now + (unsigned long long)(wd * 1e9);
+  const size_t state_bytes =
+      lead->p.precision == CCS_PREC_FP64 ? sizeof(LaneState<double>) : sizeof(LaneState<float>);
+  const size_t cap = std::min<size_t>(total, std::max<size_t>(65536, total / 4));
+  if (cap * state_bytes > lead->park_bytes) {
+    dfree(lead->d_park);
+    lead->park_bytes = 0;
+    CK(cudaMalloc(&lead->d_park, cap * state_bytes));
+    lead->park_bytes = cap * state_bytes;
+  }
+  k.park = lead->d_park;
+  k.park_cap = cap;
+  k.park_steps = lead->p.park_steps ? lead->p.park_steps : 2048u;
+  k.park_count = lead->d_work + 9;
+  k.park_next = lead->d_work + 10;
+  CK(cudaMemsetAsync(lead->d_work, 0, 8 * sizeof(unsigned long long), s));
+  CK(cudaMemsetAsync(lead->d_work + 9, 0, 2 * sizeof(unsigned long long), s));
+  CK(cudaMemsetAsync(lead->d_error, 0, sizeof(int), s));
+  lead->h_kparams = k;
+  CK(cudaMemcpyAsync(lead->d_kparams, &lead->h_kparams, sizeof(KParams), cudaMemcpyHostToDevice, s));
+  const int gas = gas_kind(lead->p.gas);
+  const bool fp64 = lead->p.precision == CCS_PREC_FP64;
+  const int Gb = batch_lanes(G);
+  KernelFn fn = fp64 ? pick_traj_batch_t<double>(gas, hasq, Gb) : pick_traj_batch_t<float>(gas, hasq, Gb);
+  KernelFn rfn = fp64 ? pick_resume_batch_t<double>(gas, hasq) : pick_resume_batch_t<float>(gas, hasq);
+  int per_sm = 0, rper_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, BLOCK, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, RBLOCK, 0));
+  size_t grid = (size_t)std::max(per_sm, 1) * lead->sm_count;
+  grid = std::min(grid, std::max<size_t>(1, (total + BLOCK - 1) / BLOCK));
+  CK(cudaEventRecord(lead->ev[5], s));
+  fn<<<(unsigned)grid, BLOCK, 0, s>>>(k, lead->d_kparams);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(lead->ev[6], s));
+  rfn<<<(unsigned)((size_t)std::max(rper_sm, 1) * lead->sm_count), RBLOCK, 0, s>>>(k, lead->d_kparams);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(lead->ev[7], s));
+  lead->last.grid_size = (int32_t)grid;
+  lead->last.block_size = BLOCK;
+  lead->last.lanes_per_traj = Gb;
+  return CCS_OK;
+}
+
+// Lanes per force evaluation for a batch: the lead's setting, else the
+// fastest of 8, 16 and 32 on a sub-batch of every ion's first trajectories.
+int autotune_batch(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const size_t *n, const size_t *off,
+                   size_t stride, int &G) {
+  ccs_ctx *c = lead;  // error reports go to the lead context
+  if (lead->p.lanes_per_traj > 0) { G = batch_lanes(lead->p.lanes_per_traj); return CCS_OK; }
+  const size_t per = std::max<size_t>(1, ((size_t)lead->sm_count * 256) / std::max<size_t>(1, nions));
+  std::vector<size_t> m(nions);
+  for (size_t i = 0; i < nions; i++) m[i] = std::min(n[i], per);
+  float best = 1e30f;
+  G = 32;
+  for (int cand : {8, 16, 32}) {
+    for (int rep = 0; rep < 2; rep++) {  // first pass warms caches and code
+      CK(cudaEventRecord(lead->ev[8], lead->stream));
+      int rc = run_batch_device(lead, ions, nions, m.data(), off, stride, false, false, cand);
+      if (rc) return rc;
+      CK(cudaEventRecord(lead->ev[9], lead->stream));
+      CK(cudaEventSynchronize(lead->ev[9]));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, lead->ev[8], lead->ev[9]));
+      if (rep == 1 && ms < best) { best = ms; G = cand; }
+    }
+  }
+  return CCS_OK;
+}
 }  // namespace
 
 // ===========================================================================
@@ -523,6 +668,7 @@ void ccs_destroy(ccs_ctx *c) {
   free_target(c);
   dfree(c->d_vtab_v); dfree(c->d_vtab_s);
   dfree(c->d_work); dfree(c->d_error); dfree(c->d_rnd); dfree(c->d_kparams); dfree(c->d_park);
+  dfree(c->d_bkp); dfree(c->d_bstart);
   dfree(c->d_key); dfree(c->d_key2); dfree(c->d_idx); dfree(c->d_idx2); dfree(c->d_sort_tmp);
   dfree(c->d_status); dfree(c->d_omc); dfree(c->d_steps); dfree(c->d_visits);
   for (auto &e : c->ev)
@@ -766,6 +912,61 @@ int ccs_run(ccs_ctx *c, size_t n, const double *const rnd[9], int8_t *status, do
   c->last.kernel_ms = t23;
   c->last.d2h_ms = t34;
   return read_stats(c, st, n);
+}
+
+int ccs_run_batch(ccs_ctx *const *ions, size_t nions, const size_t *ntraj, const double *const rnd[9],
+                  int8_t *status, double *omc, uint32_t *steps, uint32_t *visits, ccs_stats *st) {
+  if (!ions || nions == 0 || !ions[0]) return CCS_ERR_INVALID;
+  ccs_ctx *lead = ions[0];
+  if (!ntraj) return fail(lead, CCS_ERR_INVALID, "ntraj is required");
+  const int gas = gas_kind(lead->p.gas);
+  size_t total = 0;
+  std::vector<size_t> off(nions);
+  for (size_t i = 0; i < nions; i++) {
+    const ccs_ctx *ci = ions[i];
+    if (!ci) return fail(lead, CCS_ERR_INVALID, "ion %zu has no context", i);
+    if (!ci->have_target) return fail(lead, CCS_ERR_INVALID, "ion %zu has no target", i);
+    if (ci->device != lead->device) return fail(lead, CCS_ERR_INVALID, "ion %zu is on another device", i);
+    if (gas_kind(ci->p.gas) != gas) return fail(lead, CCS_ERR_INVALID, "ion %zu: atomic and molecular gases mixed", i);
+    if (ci->p.precision != lead->p.precision) return fail(lead, CCS_ERR_INVALID, "ion %zu: precision differs", i);
+    off[i] = total;
+    total += ntraj[i];
+  }
+  if (total == 0) { if (st) { std::memset(st, 0, sizeof *st); } return CCS_OK; }
+  if (!rnd || !status || !omc) return fail(lead, CCS_ERR_INVALID, "rnd, status and one_minus_cos are required");
+  const int nrows = gas == GAS_ATOM ? 5 : 9;
+  for (int k = 0; k < nrows; k++)
+    if (!rnd[k]) return fail(lead, CCS_ERR_INVALID, "rnd[%d] is NULL", k);
+  if (cudaSetDevice(lead->device) != cudaSuccess) return fail(lead, CCS_ERR_CUDA, "cudaSetDevice");
+  ccs_ctx *c = lead;  // error reports go to the lead context
+  int rc = ensure_run_buffers(lead, total, true);
+  if (rc) return rc;
+  cudaStream_t s = lead->stream;
+  CK(cudaEventRecord(lead->ev[0], s));
+  for (int k = 0; k < nrows; k++)
+    CK(cudaMemcpyAsync(lead->d_rnd + (size_t)k * total, rnd[k], total * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(lead->ev[1], s));
+  int G = 32;
+  rc = autotune_batch(lead, ions, nions, ntraj, off.data(), total, G);
+  if (rc) return rc;
+  CK(cudaEventRecord(lead->ev[2], s));
+  rc = run_batch_device(lead, ions, nions, ntraj, off.data(), total, steps != nullptr, visits != nullptr, G);
+  if (rc) return rc;
+  CK(cudaEventRecord(lead->ev[3], s));
+  CK(cudaMemcpyAsync(status, lead->d_status, total, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(omc, lead->d_omc, total * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (steps) CK(cudaMemcpyAsync(steps, lead->d_steps, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  if (visits) CK(cudaMemcpyAsync(visits, lead->d_visits, total * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaEventRecord(lead->ev[4], s));
+  CK(cudaStreamSynchronize(s));
+  float t01 = 0, t23 = 0, t34 = 0;
+  CK(cudaEventElapsedTime(&t01, lead->ev[0], lead->ev[1]));
+  CK(cudaEventElapsedTime(&t23, lead->ev[2], lead->ev[3]));
+  CK(cudaEventElapsedTime(&t34, lead->ev[3], lead->ev[4]));
+  lead->last.h2d_ms = t01;
+  lead->last.kernel_ms = t23;
+  lead->last.d2h_ms = t34;
+  return read_stats(lead, st, total);
 }
 
 int ccs_eval_site_forces(ccs_ctx *c, size_t npts, int site, const double *pos, double *f, double *U,

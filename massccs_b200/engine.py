@@ -74,7 +74,7 @@ class CcsInfo(ctypes.Structure):
 EXPORTS = ["ccs_version", "ccs_create", "ccs_destroy", "ccs_params_default", "ccs_set_target",
            "ccs_set_params", "ccs_run", "ccs_run_device", "ccs_sync_stats", "ccs_eval_site_forces",
            "ccs_eval_setup", "ccs_get_info", "ccs_status_string", "ccs_last_error",
-           "ccs_measure_fp32_peak", "ccs_run_device_noalloc"]
+           "ccs_measure_fp32_peak", "ccs_run_device_noalloc", "ccs_run_batch"]
 
 _LIB = None
 
@@ -109,6 +109,8 @@ def load_library(path=LIB_PATH):
     L.ccs_last_error.restype = ctypes.c_char_p
     L.ccs_measure_fp32_peak.argtypes = [i32, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
     L.ccs_run_device_noalloc.argtypes = [vp, sz, vp, sz, vp, vp, vp, vp, vp, ctypes.POINTER(CcsStats)]
+    L.ccs_run_batch.argtypes = [ctypes.POINTER(vp), sz, ctypes.POINTER(sz), ctypes.POINTER(vp), vp, vp, vp, vp,
+                                ctypes.POINTER(CcsStats)]
     if path == LIB_PATH:
         _LIB = L
     return L
@@ -243,6 +245,37 @@ class Engine:
         self._check(self._L.ccs_eval_setup(self._h, n, ptrs, _p(hit), _p(pos), _p(vel)),
                     "ccs_eval_setup")
         return hit, pos, vel
+
+
+def run_batch(engines, rnds, want_steps=True, want_visits=True):
+    """ccs_run_batch: every engine's ion in one launch of each pass.
+
+    engines: Engine objects (the first leads the run); rnds: one (9, n_i)
+    pre-draw per ion.  Returns one result dict per ion (as Engine.run) and the
+    run's statistics."""
+    if len(engines) != len(rnds) or not engines:
+        raise ValueError("one pre-draw per engine")
+    L = engines[0]._L
+    n = [int(r.shape[1]) for r in rnds]
+    rnd = np.ascontiguousarray(np.concatenate([np.asarray(r, dtype=np.float64) for r in rnds], axis=1))
+    total = rnd.shape[1]
+    ptrs = (ctypes.c_void_p * 9)(*[rnd[k].ctypes.data for k in range(9)])
+    hs = (ctypes.c_void_p * len(engines))(*[e._h.value for e in engines])
+    ns = (ctypes.c_size_t * len(engines))(*n)
+    status = np.empty(total, dtype=np.int8)
+    omc = np.empty(total, dtype=np.float64)
+    steps = np.empty(total, dtype=np.uint32) if want_steps else None
+    visits = np.empty(total, dtype=np.uint32) if want_visits else None
+    st = CcsStats()
+    engines[0]._check(L.ccs_run_batch(hs, len(engines), ns, ptrs, _p(status), _p(omc), _p(steps), _p(visits),
+                                      ctypes.byref(st)), "ccs_run_batch")
+    out, o = [], 0
+    for k in n:
+        out.append({"status": status[o:o + k], "one_minus_cos": omc[o:o + k],
+                    "steps": steps[o:o + k] if steps is not None else None,
+                    "visits": visits[o:o + k] if visits is not None else None})
+        o += k
+    return out, st.as_dict()
 
 
 def measure_fp32_peak(device=0, ms=200.0):
