@@ -46,6 +46,9 @@ CONFIGS = {
                        desc="1231-atom globule (Rg 11.5 A, +4 e), N2 3-site, force type 6, 3e5 trajectories"),
     "c60_he": dict(gen="c60_he", ntraj=300000, nprobe=30000, niter=10, gas="He", ft=4,
                    desc="60-atom C60 cage (C-C 1.40 A, neutral, uff.ff), He, force type 4, 3e5 trajectories"),
+    "batch_he": dict(gen="batch", gas="He", ft=4,
+                     desc="batched ions: globules of 500-50000 atoms (log-uniform), net charge 0-30 e, He, "
+                          "force type 4; one ccs_run_batch call per step"),
 }
 
 
@@ -191,6 +194,80 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_batch_bench(args, rank, world, local):
+    """batch_he: every step runs all ions through one ccs_run_batch call (host
+    buffers in and out: the call a user makes), against one ccs_run per ion."""
+    import numpy as np
+    import torch
+    from massccs_b200 import engine as E
+    from massccs_b200 import host as H
+    from massccs_b200 import synth
+    torch.cuda.set_device(local)
+    d = tempfile.mkdtemp(prefix=f"bench_batch_{rank}_")
+    t0 = time.perf_counter()
+    paths = synth.batch(d, nions=args.ions, ntraj=args.traj_per_ion, seed=2104 + 100000 * rank)
+    systems = [H.System(p) for p in paths]
+    engs = [S.engine(device=local) for S in systems]
+    rnds = [S.predraw() for S in systems]
+    natoms = [S.info["natoms"] for S in systems]
+    log(f"[rank {rank}] {len(systems)} ions, {sum(natoms)} atoms, set-up {time.perf_counter() - t0:.1f} s")
+    total = sum(r.shape[1] for r in rnds)
+    for _ in range(args.warmup):
+        E.run_batch(engs, rnds, want_steps=False, want_visits=False)
+    kern, wall, last = [], [], None
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            out, st = E.run_batch(engs, rnds, want_steps=False, want_visits=False)
+            for S, o in zip(systems, out):
+                H.reduce(S.info["niter"], S.info["nprobe"], o["status"], o["one_minus_cos"], S.info["bmax"])
+            wall.append(time.perf_counter() - t)
+            kern.append(st["kernel_ms"])
+            last = st
+    # one launch of each pass per ion (each context already tuned by a first run)
+    for e, r in zip(engs, rnds):
+        e.run(r, want_steps=False, want_visits=False)
+    t = time.perf_counter()
+    sep_kernel = 0.0
+    for e, r in zip(engs, rnds):
+        sep_kernel += e.run(r, want_steps=False, want_visits=False)["stats"]["kernel_ms"]
+    sep_wall = time.perf_counter() - t
+    ms = sum(kern) / len(kern)
+    e2e_s = sum(wall) / len(wall)
+    if rank == 0:
+        peak = E.measure_fp32_peak(local)
+        fpv = FLOPS_PER_VISIT[("He", 4)]
+        achieved = last["visits"] * fpv / (last["kernel_ms"] * 1e-3) / 1e12
+        line = {
+            "metric": METRIC + " (batched ions)", "value": world * total / (ms * 1e-3), "unit": "trajectories/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "batch_he", "description": CONFIGS["batch_he"]["desc"], "ions": len(systems),
+                       "trajectories_per_ion": args.traj_per_ion, "atoms_total": int(sum(natoms)),
+                       "atoms_min": int(min(natoms)), "atoms_max": int(max(natoms)),
+                       "l2": "no flush: each step moves 72 B per trajectory host to device (3.7e8 B at 5.12e6)"},
+            "e2e": {"value": world * total / e2e_s, "unit": "trajectories/s",
+                    "h2d_bytes_per_step": 5 * 8 * total, "d2h_bytes_per_step": 9 * total,
+                    "includes": "ccs_run_batch (H2D, both passes, D2H) and the per-ion reductions"},
+            "one_launch_per_ion": {"kernel_ms": sep_kernel, "wall_s": sep_wall,
+                                   "batch_speedup_kernel": sep_kernel / ms, "batch_speedup_wall": sep_wall / e2e_s},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if peak else None, "traffic": None,
+                         "work": f"engine candidate visits x {fpv:g} flops per visit"},
+            "cpu_baseline": None,
+            "gpu_launches": 3 * args.steps,
+            "engine": {"lane_ms": last["lane_ms"], "warp_ms": last["warp_ms"], "parked": last["parked"],
+                       "lanes_per_force": last["lanes_per_traj"]},
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    for e in engs:
+        e.close()
+    shutil.rmtree(d, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -201,6 +278,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ntraj", type=int, default=0,
                     help="trajectories per step (default: the workload's 3e5); smaller values are for profiling")
+    ap.add_argument("--ions", type=int, default=256, help="batch_he: number of ions")
+    ap.add_argument("--traj-per-ion", type=int, default=20000, help="batch_he: trajectories per ion")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -208,6 +287,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":  # CPU only: rank 0 runs it, the other ranks have nothing to do
         run_reference_arm(args, rank, world)
+        return
+    if args.config == "batch_he":
+        run_batch_bench(args, rank, world, local)
         return
     dist = None
     if world > 1:

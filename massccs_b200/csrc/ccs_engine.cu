@@ -70,6 +70,8 @@ struct ccs_ctx {
   KParams *d_bkp = nullptr;
   unsigned long long *d_bstart = nullptr;
   size_t bkp_cap = 0;
+  int batch_G = 0;                        // tuned lanes for the last batch shape
+  size_t batch_nions = 0, batch_total = 0;
   // launch choice
   int tuned_G = 0, tuned_block = 0;
   ccs_stats last{};
@@ -108,6 +110,7 @@ void free_target(ccs_ctx *c) {
   dfree(c->d_cell_start);
   c->have_target = false;
   c->tuned_G = 0;
+  c->batch_G = 0;
 }
 
 bool is_molecule(int gas) { return gas == CCS_GAS_N2 || gas == CCS_GAS_CO2; }
@@ -592,6 +595,12 @@ int autotune_batch(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const size
                    size_t stride, int &G) {
   ccs_ctx *c = lead;  // error reports go to the lead context
   if (lead->p.lanes_per_traj > 0) { G = batch_lanes(lead->p.lanes_per_traj); return CCS_OK; }
+  size_t total = 0;
+  for (size_t i = 0; i < nions; i++) total += n[i];
+  if (lead->batch_G && lead->batch_nions == nions && lead->batch_total == total) {
+    G = lead->batch_G;  // the same batch shape as last time
+    return CCS_OK;
+  }
   const size_t per = std::max<size_t>(1, ((size_t)lead->sm_count * 256) / std::max<size_t>(1, nions));
   std::vector<size_t> m(nions);
   for (size_t i = 0; i < nions; i++) m[i] = std::min(n[i], per);
@@ -609,6 +618,9 @@ int autotune_batch(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const size
       if (rep == 1 && ms < best) { best = ms; G = cand; }
     }
   }
+  lead->batch_G = G;
+  lead->batch_nions = nions;
+  lead->batch_total = total;
   return CCS_OK;
 }
 }  // namespace
@@ -819,6 +831,7 @@ int ccs_set_target(ccs_ctx *c, size_t n, const double *x, const double *y, const
   CK(cudaMemcpy(c->d_cell_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
   c->have_target = true;
   c->tuned_G = 0;
+  c->batch_G = 0;
   return CCS_OK;
 }
 

@@ -16,6 +16,10 @@ configurations the engine is measured on (sizes and distributions as stated):
              a net +40 e; He or N2; 1e6 trajectories.
   globule    N atoms, radius 1.3 N^(1/3) sqrt(5/3) A, net charge Q: the
              batched-ion and learned-field configurations.
+  batch      256 globules, N log-uniform in [500, 50000], net charge a
+             uniform integer in [0, 30] e, He, 2e4 trajectories each; the
+             minimum distance is enforced by thinning a uniform sample with
+             a k-d tree (fast_globule_atoms), not by sequential addition.
 
 Every generator writes `target.xyz` (5 columns: symbol x y z q), `uff.ff`
 when used and `input.json` into a directory and returns the json path.
@@ -176,6 +180,49 @@ def globule(d, natoms, net, gas="He", ft=None, nprobe=2000, niter=10, seed=2104,
     write_xyz(os.path.join(d, "target.xyz"), sym, xyz, q)
     ft = ft or (6 if gas in ("N2", "CO2") else 4)
     return write_input(d, "target.xyz", gas, ft, nprobe, niter, seed, extra=extra or None)
+
+
+def fast_globule_atoms(n, radius, net, rng, dmin=1.0):
+    """n atoms uniform in a sphere with no pair closer than dmin: draw 1.3 n
+    points, drop the later point of every close pair (k-d tree), keep the
+    first n survivors (redrawing if too few survive)."""
+    from scipy.spatial import cKDTree
+    m = int(1.3 * n) + 16
+    while True:
+        v = rng.normal(size=(m, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        pts = v * radius * rng.random((m, 1)) ** (1 / 3)
+        pairs = cKDTree(pts).query_pairs(dmin, output_type="ndarray")
+        keep = np.ones(m, dtype=bool)
+        keep[pairs.max(axis=1)] = False
+        # a point dropped for one pair may leave its partner in another close pair: thin again
+        idx = np.flatnonzero(keep)
+        sub = pts[idx]
+        pairs = cKDTree(sub).query_pairs(dmin, output_type="ndarray")
+        if len(pairs):
+            k2 = np.ones(len(idx), dtype=bool)
+            k2[pairs.max(axis=1)] = False
+            idx = idx[k2]
+        if len(idx) >= n:
+            xyz = pts[idx[:n]]
+            return _elements(n, rng), xyz, _charges(n, net, rng)
+        m = int(m * 1.3)
+
+
+def batch(d, nions=256, ntraj=20000, nmin=500, nmax=50000, qmax=30, seed=2104, gen_seed=256):
+    """The batched-ion workload: one directory (and input.json) per ion; returns the json paths."""
+    rng = np.random.default_rng(gen_seed)
+    sizes = np.exp(rng.uniform(np.log(nmin), np.log(nmax), nions)).astype(int)
+    charges = rng.integers(0, qmax + 1, nions)
+    paths = []
+    for i, (n, q) in enumerate(zip(sizes, charges)):
+        di = os.path.join(d, f"ion{i:03d}")
+        os.makedirs(di, exist_ok=True)
+        radius = 1.3 * n ** (1 / 3) * (5 / 3) ** 0.5
+        sym, xyz, qq = fast_globule_atoms(int(n), radius, float(q), rng)
+        write_xyz(os.path.join(di, "target.xyz"), sym, xyz, qq)
+        paths.append(write_input(di, "target.xyz", "He", 4, ntraj, 1, seed + i))
+    return paths
 
 
 def shell(d, natoms=500000, r_in=100.0, r_out=130.0, net=40.0, gas="He", nprobe=100000, niter=10, seed=2104,
