@@ -847,6 +847,18 @@ template <typename T> __device__ __forceinline__ bool outside_box(const KParams 
 // kept.
 enum : int { M_IDLE = 0, M_INIT = 1, M_RESTART = 2, M_STEP = 3 };
 constexpr int BLOCK = 128;
+// Resident CTAs per SM the register allocation must allow.  Lane pass: 3.
+// Warp pass: molecules run 512 threads per SM (8 CTAs of 64 at <= 128
+// registers; measured 2.58 -> 2.07 s on the 1231-atom N2 workload, whose
+// warp pass is throughput-bound), atoms are left unconstrained (their warp
+// pass is bound by the latency of the longest trajectory), and so is the
+// FP64 parity mode (128 registers would spill).
+#ifndef CCS_LANE_MIN_BLOCKS
+#define CCS_LANE_MIN_BLOCKS 3
+#endif
+#ifndef CCS_WARP_MIN_BLOCKS
+#define CCS_WARP_MIN_BLOCKS(T, nt, gas) ((gas) == GAS_ATOM || sizeof(T) == 8 ? 1 : 512 / (nt))
+#endif
 
 __device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
   for (int k = 0; k < n; k++) m &= m - 1u;
@@ -1140,7 +1152,7 @@ __device__ __forceinline__ const KParams *ion_params_ptr(const KParams &kp, cons
 }
 
 template <typename T, int G, int GAS, bool HASQ, bool BATCH>
-__global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParams *__restrict__ kpg) {
+__global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParams kp, const KParams *__restrict__ kpg) {
   using S = Sites<GAS>;
   constexpr int NS = S::NS;
   constexpr int NSUB = 32 / G;
@@ -1328,7 +1340,7 @@ __global__ void __launch_bounds__(BLOCK, 3) traj_kernel(KParams kp, const KParam
 constexpr int RBLOCK = 64;  // default threads per trajectory in the warp pass
 
 template <typename T, int GAS, bool HASQ, int NT, bool BATCH>
-__global__ void __launch_bounds__(NT) resume_kernel(KParams kp, const KParams *__restrict__ kpg) {
+__global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_kernel(KParams kp, const KParams *__restrict__ kpg) {
   using S = Sites<GAS>;
   constexpr int NS = S::NS;
   __shared__ int sm_list[LCAP], sm_wsum[NT / 32];
