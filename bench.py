@@ -18,6 +18,9 @@ roofline   FP32-pipe roofline of the trajectory kernels: algorithmic flops (the
            the device time, against the device's measured FP32 FMA peak
 cpu_baseline  the reference binary (oracle/_ref/massccs) on this host's cores,
            on a bounded sample of the same workload
+accuracy   the metric's condition: the FP32 CCS against the engine's FP64
+           mode on the first 2e4 trajectories of the same initial conditions
+           (paired relative difference and its standard error)
 """
 import argparse
 import json
@@ -159,6 +162,28 @@ def cpu_baseline(json_path, config):
     return out, visits
 
 
+def fp64_check(S, eng, rnd, status, omc, m, device):
+    """The metric's accuracy condition: the first m trajectories of the last
+    end-to-end step rerun in the engine's FP64 mode on the same initial
+    conditions; CCS estimate = mean dOmega over free + scatter (the reference's
+    estimator), paired difference and its standard error."""
+    import numpy as np
+    m = min(m, rnd.shape[1])
+    e64 = S.engine(device=device, precision=1)
+    r64 = e64.run(np.ascontiguousarray(rnd[:, :m]), want_steps=False, want_visits=False)
+    e64.close()
+    bmax = S.info["bmax"]
+    a = np.pi * np.where(r64["status"] == 1, r64["one_minus_cos"], 0.0) * bmax ** 2
+    b = np.pi * np.where(status[:m] == 1, omc[:m], 0.0) * bmax ** 2
+    ok = (r64["status"] <= 1) & (status[:m] <= 1)
+    ref = float(a[ok].mean())
+    d = (b - a)[ok]
+    return {"vs": "FP64 engine mode on the same initial conditions (paired)", "trajectories": int(m),
+            "ccs_fp64_A2": ref, "ccs_fp32_A2": float(b[ok].mean()), "rel_diff": float(d.mean() / ref),
+            "rel_se": float(d.std(ddof=1) / np.sqrt(len(d)) / ref),
+            "status_agreement": float((r64["status"] == status[:m]).mean())}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -278,6 +303,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ntraj", type=int, default=0,
                     help="trajectories per step (default: the workload's 3e5); smaller values are for profiling")
+    ap.add_argument("--fp64-check", type=int, default=20000,
+                    help="trajectories rerun in FP64 mode to report the FP32 CCS error (0: skip)")
     ap.add_argument("--ions", type=int, default=256, help="batch_he: number of ions")
     ap.add_argument("--traj-per-ion", type=int, default=20000, help="batch_he: trajectories per ion")
     args = ap.parse_args()
@@ -399,6 +426,7 @@ def main():
     if rank == 0:
         status = st_pin
         nscatter = int((status == 1).sum())
+        accuracy = fp64_check(S, eng, pin_np, st_pin, om_pin, args.fp64_check, local) if args.fp64_check else None
         peak = E.measure_fp32_peak(local)
         engine_visits = last["visits"] / max(1, n)
         ref_visits = None
@@ -432,6 +460,7 @@ def main():
                          "engine_visits_per_traj": engine_visits,
                          "engine_tflops": n * engine_visits * fpv / kernel_s / 1e12},
             "cpu_baseline": cpu,
+            "accuracy": accuracy,
             "gpu_launches": 3 * args.steps,
             "engine": {"lane_ms": last["lane_ms"], "warp_ms": last["warp_ms"], "parked": last["parked"],
                        "lanes_per_force": last["lanes_per_traj"], "scatter_fraction": nscatter / n,

@@ -87,7 +87,7 @@ typedef struct {
   int32_t precision;        /* ccs_precision */
   int32_t quirks;           /* CCS_QUIRK_* bits */
   double cell_size;         /* engine cell edge in A; 0 = automatic */
-  int32_t lanes_per_traj;   /* 0 = autotuned, else 1,2,4,8,16 or 32 lanes per trajectory */
+  int32_t lanes_per_traj;   /* 0 = autotuned, else 1, 4, 8, 16 or 32 lanes per force evaluation */
   int32_t block_size;       /* 0 = automatic (multiple of 32) */
   uint32_t max_steps_per_try; /* 0 = 2,000,000 */
   double watchdog_s;        /* kernel wall-time budget, 0 = 600 s */

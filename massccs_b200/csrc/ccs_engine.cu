@@ -176,7 +176,6 @@ int g_index(int G) { int i = 0; while ((1 << i) < G) i++; return i; }
 template <typename T, int GAS, bool HASQ> KernelFn pick_traj_g(int gi) {
   switch (gi) {
     case 0: return traj_ptr<T, 1, GAS, HASQ>();
-    case 1:
     case 2: return traj_ptr<T, 4, GAS, HASQ>();
     case 3: return traj_ptr<T, 8, GAS, HASQ>();
     case 4: return traj_ptr<T, 16, GAS, HASQ>();
@@ -705,8 +704,8 @@ int ccs_set_params(ccs_ctx *c, const ccs_params *p) {
   if (p->precision != CCS_PREC_FP32 && p->precision != CCS_PREC_FP64)
     return fail(c, CCS_ERR_INVALID, "precision must be FP32 or FP64");
   const int G = p->lanes_per_traj;
-  if (G != 0 && G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32)
-    return fail(c, CCS_ERR_INVALID, "lanes_per_traj must be 0 or a power of two up to 32");
+  if (G != 0 && G != 1 && G != 4 && G != 8 && G != 16 && G != 32)
+    return fail(c, CCS_ERR_INVALID, "lanes_per_traj must be 0, 1, 4, 8, 16 or 32");
   if (p->block_size != 0 && p->block_size != BLOCK)
     return fail(c, CCS_ERR_INVALID, "block_size must be 0 or %d", BLOCK);
   if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");

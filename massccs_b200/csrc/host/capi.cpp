@@ -2,6 +2,7 @@
 // mh_run: the reference's whole run (System.cpp:19-326) with the trajectory
 // loop replaced by ccs_run.
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <iostream>
@@ -183,6 +184,44 @@ int mh_run(mh_system *sys, int device, const ccs_params *overrides, int print, d
     if (st.ncapped)
       std::cout << "warning: " << st.ncapped << " trajectories reached the step cap and were counted as lost"
                 << std::endl;
+  }
+  // The FP32 result's error against FP64: the first trajectories again in the
+  // engine's FP64 mode on the same initial conditions, compared pairwise
+  // (dOmega of free and scattered trajectories, the reference's estimator).
+  const size_t m = std::min<size_t>(n, S.in.fp64_check);
+  if (print && m > 1 && p.precision == CCS_PREC_FP32) {
+    ccs_params p64 = p;
+    p64.precision = CCS_PREC_FP64;
+    std::vector<int8_t> st64(m);
+    std::vector<double> om64(m);
+    ccs_stats s64;
+    if ((rc = ccs_set_params(ctx, &p64)) ||
+        (rc = ccs_set_target(ctx, (size_t)S.target.natoms, S.target.x.data(), S.target.y.data(), S.target.z.data(),
+                             S.target.q.data(), S.target.eps.data(), S.target.sig.data(),
+                             S.in.gas_buffer_flag == 3 ? S.target.eps_c.data() : nullptr,
+                             S.in.gas_buffer_flag == 3 ? S.target.sig_c.data() : nullptr)) ||
+        (rc = ccs_run(ctx, m, rows, st64.data(), om64.data(), nullptr, nullptr, &s64))) {
+      std::cerr << "massccs: FP64 check: " << ccs_last_error(ctx) << std::endl;
+      return rc;
+    }
+    const double w = M_PI * S.bmax * S.bmax;
+    double sa = 0, sb = 0, sd = 0, sdd = 0;
+    size_t k = 0, agree = 0;
+    for (size_t j = 0; j < m; j++) {
+      agree += st64[j] == status[j];
+      if (st64[j] > 1 || status[j] > 1) continue;  // lost in either: outside the estimator
+      const double a = st64[j] == 1 ? w * om64[j] : 0.0, b = status[j] == 1 ? w * omc[j] : 0.0;
+      sa += a; sb += b; sd += b - a; sdd += (b - a) * (b - a);
+      k++;
+    }
+    if (k > 1 && sa > 0) {
+      const double mean_d = sd / k, var = (sdd - k * mean_d * mean_d) / (k - 1);
+      std::printf("FP64 check: the first %zu trajectories again in FP64: CCS %.6g (FP32) vs %.6g (FP64) Ang^2, "
+                  "relative difference %+.3f %% +- %.3f %% (paired), status agreement %.2f %%\n",
+                  m, sb / k, sa / k, 100.0 * mean_d / (sa / k), 100.0 * std::sqrt(std::max(var, 0.0) / k) / (sa / k),
+                  100.0 * agree / m);
+      std::fflush(stdout);
+    }
   }
   if (ccs_out) *ccs_out = R.ccs;
   if (err_out) *err_out = R.err;

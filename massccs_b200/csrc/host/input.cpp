@@ -137,6 +137,7 @@ Input::Input(const std::string &path) {
     if (precision != "fp32" && precision != "fp64")
       throw std::invalid_argument("precision must be fp32 or fp64");
   }
+  if (has("fp64_check")) fp64_check = unsigned_number(d["fp64_check"], "fp64_check");
 }
 
 void Input::print() const {

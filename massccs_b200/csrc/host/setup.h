@@ -23,6 +23,7 @@ struct Input {
               polar_str = "yes";
   bool ref_quirks = false;   // extension key "ref_quirks": reproduce the CO2 reference-velocity bug
   std::string precision = "fp32";  // extension key "precision": "fp32" or "fp64"
+  unsigned fp64_check = 2000;      // extension key "fp64_check": FP32 runs rerun this many trajectories in FP64
 
   explicit Input(const std::string &path);
   void print() const;  // Input::printReadInput (Input.cpp:313-345)

@@ -166,3 +166,16 @@ def test_watchdog_expiry_is_an_error_and_the_context_survives(oracle):
     out = eng.run(rnd[:, :400])
     assert out["stats"]["ncapped"] == 0
     assert (out["status"] <= 1).mean() > 0.9
+
+
+def test_co2_reference_velocity_quirk_matches_oracle(oracle):
+    """CCS_QUIRK_CO2_VCM reproduces the reference's CO2 initial-velocity slip
+    (System.cpp:1012): FP64 engine and oracle agree with the quirk on, and the
+    quirk changes the scattering angles (it is not a no-op)."""
+    s, ref, out = _paired(oracle, "c60.xyz", "CO2", 4, 400, prec=1, quirks=1)
+    same = out["status"] == ref["status"]
+    close = same & (np.abs(out["one_minus_cos"] - ref["one_minus_cos"]) <= 1e-7)
+    assert close.mean() >= 0.97, close.mean()
+    plain = engine_for(s, precision=1, quirks=0).run(s.predraw(400))
+    sc = (plain["status"] == 1) & (out["status"] == 1)
+    assert np.abs(plain["one_minus_cos"][sc] - out["one_minus_cos"][sc]).max() > 1e-3
