@@ -19,8 +19,8 @@ roofline   FP32-pipe roofline of the trajectory kernels: algorithmic flops (the
 cpu_baseline  the reference binary (oracle/_ref/massccs) on this host's cores,
            on a bounded sample of the same workload
 accuracy   the metric's condition: the FP32 CCS against the engine's FP64
-           mode on the first 2e4 trajectories of the same initial conditions
-           (paired relative difference and its standard error)
+           mode on the same initial conditions (all of the step's trajectories
+           by default; paired relative difference and its standard error)
 """
 import argparse
 import json
@@ -303,8 +303,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ntraj", type=int, default=0,
                     help="trajectories per step (default: the workload's 3e5); smaller values are for profiling")
-    ap.add_argument("--fp64-check", type=int, default=20000,
-                    help="trajectories rerun in FP64 mode to report the FP32 CCS error (0: skip)")
+    ap.add_argument("--fp64-check", type=int, default=-1,
+                    help="trajectories rerun in FP64 mode to report the FP32 CCS error (-1: all, 0: skip)")
     ap.add_argument("--ions", type=int, default=256, help="batch_he: number of ions")
     ap.add_argument("--traj-per-ion", type=int, default=20000, help="batch_he: trajectories per ion")
     args = ap.parse_args()
@@ -426,7 +426,8 @@ def main():
     if rank == 0:
         status = st_pin
         nscatter = int((status == 1).sum())
-        accuracy = fp64_check(S, eng, pin_np, st_pin, om_pin, args.fp64_check, local) if args.fp64_check else None
+        m = n if args.fp64_check < 0 else args.fp64_check
+        accuracy = fp64_check(S, eng, pin_np, st_pin, om_pin, m, local) if m > 0 else None
         peak = E.measure_fp32_peak(local)
         engine_visits = last["visits"] / max(1, n)
         ref_visits = None

@@ -94,6 +94,8 @@ typedef struct {
   int32_t schedule;         /* 0 = index order, 1 = longest expected trajectories first */
   uint32_t park_steps;      /* steps after which a trajectory moves to the warp pass; 0 = 2048 */
   int32_t resume_block;     /* threads per trajectory in the warp pass: 32, 64 or 128; 0 = 64 */
+  int32_t spec_tries;       /* failed tries after which a warp-pass trajectory runs its remaining
+                               tries at once (2..8); 0 = default, < 0 = never */
 } ccs_params;
 
 /* Per-run statistics. */
@@ -104,7 +106,8 @@ typedef struct {
   uint64_t parked;          /* trajectories finished by the warp pass (the long ones) */
   double kernel_ms;         /* device time of both trajectory passes (CUDA events) */
   double h2d_ms, d2h_ms;    /* copy times of ccs_run (CUDA events) */
-  int32_t lanes_per_traj, block_size, grid_size, reserved;
+  int32_t lanes_per_traj, block_size, grid_size;
+  int32_t speculated;       /* warp-pass trajectories whose remaining tries ran at once */
   double lane_ms, warp_ms;  /* the lane pass and the warp pass separately */
 } ccs_stats;
 

@@ -92,6 +92,17 @@ struct KParams {
   const struct KParams *ions;
   const unsigned long long *ion_start;
   int nions;
+  // speculative retries (see resume_kernel): records of trajectories that
+  // failed their second try in the warp pass, the outcome of each remaining
+  // try, and the phase of the warp-pass launch (0: parked trajectories,
+  // 1: the speculative tries); spec_rec == nullptr: no speculation
+  struct SpecRec *spec_rec;
+  struct SpecOut *spec_out;
+  unsigned long long *spec_count, *spec_next;
+  unsigned long long spec_cap;
+  int spec_phase;
+  int spec_from;  // failed tries after which a warp-pass trajectory is handed over
+  unsigned long long spec_max_parked;  // speculate only when at most this many were parked
   int *error;                 // 1 = watchdog
 };
 
@@ -100,6 +111,25 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+
+// A trajectory handed to the speculative phase: it failed try tries - 1 and
+// will run tries tries..8 (the reference never runs a tenth: tries < maxTries
+// <= 9), all at once, one CTA each.
+struct SpecRec {
+  double Ei;                  // initial total energy (the same for every try)
+  unsigned long long j;
+  uint32_t ion, nsteps, nvis; // steps and visits of the tries before
+  int tries, maxTries;
+};
+// The end of one speculative try: 1 scatter (omc valid), 3 capped or watchdog,
+// 4 failed the angle test, 5 failed the energy test.
+struct SpecOut {
+  double omc;
+  uint32_t steps, nvis;
+  int code, pad;
+};
+constexpr int SPEC_FROM_MIN = 2;  // the fewest failed tries after which speculation starts
+constexpr int SPEC_SLOTS = 9 - SPEC_FROM_MIN;  // tries tries..tries+6 (those above 8 are skipped)
 
 template <typename T> struct Real;
 template <> struct Real<float> {
@@ -1337,6 +1367,18 @@ __global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParam
 
 // Warp pass: parked trajectories resume one per CTA (all NT threads hold
 // the same state; the force phase is block-cooperative).
+//
+// Speculative retries.  A failed try restarts the trajectory from its
+// initial state with the step dt0/(k+1) (System.cpp:453-458); the tries of a
+// trajectory are therefore independent computations, and only the decision
+// which one counts is sequential.  Captured orbits fail try after try, each
+// longer than the last, and set the end of a run.  So once a warp-pass
+// trajectory has failed spec_from tries (phase 0), it is recorded and left;
+// a second launch (phase 1) runs each recorded trajectory's remaining tries
+// at once, one CTA each, from the same code; spec_resolve_kernel then walks
+// every record's tries in order with the reference's rules.  Every try runs
+// the same instructions as it would in sequence, so the results are those of
+// the sequential path.
 constexpr int RBLOCK = 64;  // default threads per trajectory in the warp pass
 
 template <typename T, int GAS, bool HASQ, int NT, bool BATCH>
@@ -1350,52 +1392,101 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
   if (threadIdx.x < 8) blk[threadIdx.x] = 0ull;
   __syncthreads();
   const int tid = threadIdx.x;
-  unsigned long long np = *(volatile unsigned long long *)kp.park_count;
-  if (np > kp.park_cap) np = kp.park_cap;
+  const bool spec = kp.spec_phase != 0;
+  unsigned long long np;
+  if (spec) {
+    np = *(volatile unsigned long long *)kp.spec_count;
+    if (np > kp.spec_cap) np = kp.spec_cap;
+    np *= SPEC_SLOTS;
+  } else {
+    np = *(volatile unsigned long long *)kp.park_count;
+    if (np > kp.park_cap) np = kp.park_cap;
+  }
+  unsigned long long *next = spec ? kp.spec_next : kp.park_next;
+  // speculation pays when the warp pass is bound by its longest chains of
+  // tries, not when parked trajectories outnumber the CTAs (then the extra
+  // tries only add work)
+  const bool may_spec = kp.spec_rec && !spec && np <= kp.spec_max_parked;
   for (;;) {
-    if (tid == 0) sm_idx = *(volatile int *)kp.error ? np : atomicAdd(kp.park_next, 1ull);
+    if (tid == 0) sm_idx = *(volatile int *)kp.error ? np : atomicAdd(next, 1ull);
     __syncthreads();
     const unsigned long long idx = sm_idx;
     __syncthreads();
     if (idx >= np) break;
-    LaneState<T> L = reinterpret_cast<const LaneState<T> *>(kp.park)[idx];
+    LaneState<T> L;
+    unsigned long long rec = 0;
+    if (spec) {  // try k of record rec, from the trajectory's initial state
+      rec = idx / SPEC_SLOTS;
+      const SpecRec R = kp.spec_rec[rec];
+      const int k = R.tries + (int)(idx % SPEC_SLOTS);
+      if (k > 8) continue;  // beyond the reference's last try (block-uniform)
+      L.j = R.j;
+      L.ion = R.ion;
+      load_init<T, GAS>(L, lane_setup<T, GAS>(ion_params_ptr<BATCH>(kp, kpg, L.ion), L.j));
+      L.Ei = T(R.Ei);
+      L.tries = k;
+      L.maxTries = R.maxTries;
+      L.dt = T(ion_params<BATCH>(kp, L.ion).dt / (k + 1));
+      L.mode = M_RESTART;
+      L.nsteps = 0;
+      L.nvis = 0;
+    } else {
+      L = reinterpret_cast<const LaneState<T> *>(kp.park)[idx];
+    }
     const KParams &K = ion_params<BATCH>(kp, L.ion);
     const KParams *Kg = ion_params_ptr<BATCH>(kp, kpg, L.ion);
     int list_n = -1;  // this trajectory's candidate list (none yet)
     T list_c[3] = {T(0), T(0), T(0)};
     for (unsigned it = 1;; it++) {
+      int r = S_CONTINUE;
+      double omc = 0.0;
       if ((it & 1023u) == 0) {
         if (tid == 0) sm_idx = (global_ns() > kp.deadline_ns || *(volatile int *)kp.error) ? 1ull : 0ull;
         __syncthreads();
         const bool e = sm_idx != 0;
         __syncthreads();
         if (e) {
-          if (tid == 0) { atomicExch(kp.error, 1); write_result(K, L, 3, 0.0, blk); }
-          break;
+          if (tid == 0) atomicExch(kp.error, 1);
+          r = S_CAPPED;
         }
       }
-      if (L.mode == M_STEP) first_half<T, GAS>(K, L);
-      T p[NS][3], fs[NS][3], Us[NS];
-      site_positions<T, GAS>(L, p);
-      unsigned actbits;
-      if (probe_near<T, GAS>(K, p, actbits)) {
-        bool act[NS];
+      if (r == S_CONTINUE) {
+        if (L.mode == M_STEP) first_half<T, GAS>(K, L);
+        T p[NS][3], fs[NS][3], Us[NS];
+        site_positions<T, GAS>(L, p);
+        unsigned actbits;
+        if (probe_near<T, GAS>(K, p, actbits)) {
+          bool act[NS];
 #pragma unroll
-        for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
-        eval_forces_block<T, NT, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
-                                              tid, sm_list, sm_wsum, sm_red, list_n, list_c, Kg);
-      } else {
+          for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
+          eval_forces_block<T, NT, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
+                                                tid, sm_list, sm_wsum, sm_red, list_n, list_c, Kg);
+        } else {
 #pragma unroll
-        for (int s = 0; s < NS; s++) fs[s][0] = fs[s][1] = fs[s][2] = Us[s] = T(0);
+          for (int s = 0; s < NS; s++) fs[s][0] = fs[s][1] = fs[s][2] = Us[s] = T(0);
+        }
+        absorb_forces<T, GAS>(K, fs, Us, L);
+        if (L.mode == M_INIT) { L.Ei += L.U; L.mode = M_STEP; continue; }
+        if (L.mode == M_RESTART) { L.mode = M_STEP; continue; }
+        T vc[3];
+        r = second_half<T, GAS>(K, L, vc);
+        if (r == S_CONTINUE) continue;
+        if (r == S_SCATTER) omc = lane_chi<T, GAS>(Kg, L.j, vc[0], vc[1], vc[2]);
       }
-      absorb_forces<T, GAS>(K, fs, Us, L);
-      if (L.mode == M_INIT) { L.Ei += L.U; L.mode = M_STEP; continue; }
-      if (L.mode == M_RESTART) { L.mode = M_STEP; continue; }
-      T vc[3];
-      const int r = second_half<T, GAS>(K, L, vc);
-      if (r == S_CONTINUE) continue;
+      // the try has ended: scatter, capped (or watchdog), or a failed test
+      if (spec) {
+        if (tid == 0) {
+          SpecOut o;
+          o.omc = omc;
+          o.steps = L.nsteps;
+          o.nvis = L.nvis;
+          o.code = r == S_SCATTER ? 1 : r == S_CAPPED ? 3 : r == S_RETRY_ANGLE ? 4 : 5;
+          o.pad = 0;
+          kp.spec_out[rec * SPEC_SLOTS + (L.tries - kp.spec_rec[rec].tries)] = o;
+        }
+        break;
+      }
       if (r == S_SCATTER) {
-        const double omc = lane_chi<T, GAS>(Kg, L.j, vc[0], vc[1], vc[2]);
         if (tid == 0) write_result(K, L, 1, omc, blk);
         break;
       }
@@ -1410,11 +1501,75 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
         if (tid == 0) write_result(K, L, 2, 0.0, blk);
         break;
       }
+      if (may_spec && L.tries >= kp.spec_from) {  // hand the remaining tries to the speculative phase
+        if (tid == 0) {
+          const unsigned long long slot = atomicAdd(kp.spec_count, 1ull);
+          sm_idx = slot;
+          if (slot < kp.spec_cap) {
+            SpecRec R;
+            R.Ei = (double)L.Ei;
+            R.j = L.j;
+            R.ion = L.ion;
+            R.nsteps = L.nsteps;
+            R.nvis = L.nvis;
+            R.tries = L.tries;
+            R.maxTries = L.maxTries;
+            kp.spec_rec[slot] = R;
+          }
+        }
+        __syncthreads();
+        const bool recorded = sm_idx < kp.spec_cap;
+        __syncthreads();
+        if (recorded) break;
+      }
       load_init<T, GAS>(L, lane_setup<T, GAS>(Kg, L.j));
       L.mode = M_RESTART;
       list_n = -1;
     }
     __syncthreads();
+  }
+  __syncthreads();
+  if (threadIdx.x < 6 && blk[threadIdx.x]) atomicAdd(&kp.stats[threadIdx.x], blk[threadIdx.x]);
+}
+
+// The speculative tries' verdict, one thread per record: the tries in order,
+// with the reference's rules (System.cpp:453-473): a failed energy test
+// grants one more try, at most 9 tries and 2 such grants; the first try that
+// scatters decides.  Steps and visits add up over the tries that ran in
+// sequence (those after the deciding one are not counted).  After a
+// watchdog stop every record is reported capped.
+template <bool BATCH>
+__global__ void spec_resolve_kernel(KParams kp) {
+  __shared__ unsigned long long blk[8];
+  if (threadIdx.x < 8) blk[threadIdx.x] = 0ull;
+  __syncthreads();
+  unsigned long long n = *(volatile unsigned long long *)kp.spec_count;
+  if (n > kp.spec_cap) n = kp.spec_cap;
+  const unsigned long long r = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < n) {
+    const SpecRec R = kp.spec_rec[r];
+    const KParams &K = ion_params<BATCH>(kp, R.ion);
+    const bool stopped = *(volatile int *)kp.error != 0;
+    uint32_t steps = R.nsteps, nvis = R.nvis;
+    int tries = R.tries, maxTries = R.maxTries, st = stopped ? 3 : 2;
+    double omc = 0.0;
+    for (int k = R.tries; k <= 8 && !stopped; k++) {
+      const SpecOut o = kp.spec_out[r * SPEC_SLOTS + (k - R.tries)];
+      steps += o.steps;
+      nvis += o.nvis;
+      if (o.code == 1) { st = 1; omc = o.omc; break; }
+      if (o.code == 3) { st = 3; break; }
+      tries = k + 1;
+      if (o.code == 5) maxTries++;
+      if (!(tries < maxTries && maxTries < 10)) { st = 2; break; }
+    }
+    K.status[R.j] = (int8_t)st;
+    K.omc[R.j] = st == 1 ? omc : 0.0;
+    if (K.steps) K.steps[R.j] = steps;
+    if (K.visits) K.visits[R.j] = nvis;
+    atomicAdd(&blk[st], 1ull);
+    atomicAdd(&blk[4], (unsigned long long)steps);
+    atomicAdd(&blk[5], (unsigned long long)nvis);
   }
   __syncthreads();
   if (threadIdx.x < 6 && blk[threadIdx.x]) atomicAdd(&kp.stats[threadIdx.x], blk[threadIdx.x]);

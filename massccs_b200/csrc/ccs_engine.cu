@@ -63,6 +63,10 @@ struct ccs_ctx {
   // parked long trajectories (lane pass -> warp pass)
   void *d_park = nullptr;
   size_t park_bytes = 0;
+  // speculative retries: records and try outcomes
+  SpecRec *d_spec_rec = nullptr;
+  SpecOut *d_spec_out = nullptr;
+  size_t spec_cap = 0;
   // device copy of the launch parameters (read by the non-inlined set-up code)
   KParams *d_kparams = nullptr;
   KParams h_kparams{};
@@ -303,6 +307,48 @@ KParams base_params(const ccs_ctx *c) {
   return k;
 }
 
+// Speculative-retry buffers for up to cap records (the park capacity) and
+// the counters d_work[11] (records) and d_work[12] (next speculative try).
+int setup_spec(ccs_ctx *c, KParams &k, size_t cap, cudaStream_t s) {
+  if (cap > c->spec_cap) {
+    dfree(c->d_spec_rec); dfree(c->d_spec_out);
+    c->spec_cap = 0;
+    CK(cudaMalloc(&c->d_spec_rec, cap * sizeof(SpecRec)));
+    CK(cudaMalloc(&c->d_spec_out, cap * SPEC_SLOTS * sizeof(SpecOut)));
+    c->spec_cap = cap;
+  }
+  k.spec_rec = c->d_spec_rec;
+  k.spec_out = c->d_spec_out;
+  k.spec_count = c->d_work + 11;
+  k.spec_next = c->d_work + 12;
+  k.spec_cap = cap;
+  k.spec_phase = 0;
+  k.spec_from = std::max(SPEC_FROM_MIN, c->p.spec_tries > 0 ? c->p.spec_tries : 2);
+  if (c->p.spec_tries < 0) k.spec_rec = nullptr;  // speculation off
+  CK(cudaMemsetAsync(c->d_work + 11, 0, 2 * sizeof(unsigned long long), s));
+  return CCS_OK;
+}
+
+// The warp pass: parked trajectories (phase 0), the speculative tries of
+// those that failed spec_from tries there (phase 1), their verdicts.
+template <bool BATCH>
+int launch_warp_pass(ccs_ctx *c, KernelFn rfn, int rnt, KParams k, cudaStream_t s) {
+  int rper_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, rnt, 0));
+  const unsigned rgrid = (unsigned)((size_t)std::max(rper_sm, 1) * c->sm_count);
+  k.spec_max_parked = 2ull * rgrid;  // measured: 448 parked of 3e5 (60 atoms, He) 1.7x faster, 52,241 (1231 atoms, N2) slower
+  rfn<<<rgrid, rnt, 0, s>>>(k, c->d_kparams);
+  CK(cudaGetLastError());
+  if (k.spec_rec) {
+    k.spec_phase = 1;
+    rfn<<<rgrid, rnt, 0, s>>>(k, c->d_kparams);
+    CK(cudaGetLastError());
+    spec_resolve_kernel<BATCH><<<(unsigned)((k.spec_cap + 255) / 256), 256, 0, s>>>(k);
+    CK(cudaGetLastError());
+  }
+  return CCS_OK;
+}
+
 int ensure_run_buffers(ccs_ctx *c, size_t n, bool need_rnd) {
   if (need_rnd && n > c->rnd_cap) {
     dfree(c->d_rnd);
@@ -397,7 +443,10 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   k.park_steps = c->p.park_steps ? c->p.park_steps : 2048u;
   k.park_count = c->d_work + 9;
   k.park_next = c->d_work + 10;
-  // d_work: [0] work counter, [1..7] statistics, [8] clock scratch, [9] parked, [10] resumed
+  rc = setup_spec(c, k, cap, s);
+  if (rc) return rc;
+  // d_work: [0] work counter, [1..7] statistics, [8] clock scratch, [9] parked, [10] resumed,
+  // [11] speculative records, [12] next speculative try
   CK(cudaMemsetAsync(c->d_work, 0, 8 * sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(c->d_work + 9, 0, 2 * sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(c->d_error, 0, sizeof(int), s));
@@ -408,13 +457,8 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev[6], s));
   // warp pass over the parked trajectories (exits at once when none were parked)
-  KernelFn rfn = pick_resume(c);
-  int rper_sm = 0;
-  const int rnt = resume_threads(c);
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, rnt, 0));
-  if (rper_sm < 1) rper_sm = 1;
-  rfn<<<(unsigned)((size_t)rper_sm * c->sm_count), rnt, 0, s>>>(k, c->d_kparams);
-  CK(cudaGetLastError());
+  rc = launch_warp_pass<false>(c, pick_resume(c), resume_threads(c), k, s);
+  if (rc) return rc;
   CK(cudaEventRecord(c->ev[7], s));
   c->last.grid_size = (int32_t)grid;
   c->last.block_size = block;
@@ -423,7 +467,7 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
 }
 
 int read_stats(ccs_ctx *c, ccs_stats *st, size_t n) {
-  unsigned long long h[7];
+  unsigned long long h[12];  // d_work[1..12]: statistics, clock, park and speculation counters
   int herr = 0;
   {
     float a = 0, b = 0;
@@ -439,6 +483,7 @@ int read_stats(ccs_ctx *c, ccs_stats *st, size_t n) {
   c->last.ntraj = n;
   c->last.nfree = h[0]; c->last.nscatter = h[1]; c->last.nlost = h[2]; c->last.ncapped = h[3];
   c->last.steps = h[4]; c->last.visits = h[5]; c->last.parked = h[6];
+  c->last.speculated = (int32_t)std::min<unsigned long long>(h[10], c->spec_cap);
   if (st) *st = c->last;
   if (herr) return fail(c, CCS_ERR_TIMEOUT, "device watchdog expired after %.0f s",
                         c->p.watchdog_s > 0 ? c->p.watchdog_s : 600.0);
@@ -560,6 +605,8 @@ int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const si
   k.park_steps = lead->p.park_steps ? lead->p.park_steps : 2048u;
   k.park_count = lead->d_work + 9;
   k.park_next = lead->d_work + 10;
+  rc = setup_spec(lead, k, cap, s);
+  if (rc) return rc;
   CK(cudaMemsetAsync(lead->d_work, 0, 8 * sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(lead->d_work + 9, 0, 2 * sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(lead->d_error, 0, sizeof(int), s));
@@ -570,17 +617,16 @@ int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const si
   const int Gb = batch_lanes(G);
   KernelFn fn = fp64 ? pick_traj_batch_t<double>(gas, hasq, Gb) : pick_traj_batch_t<float>(gas, hasq, Gb);
   KernelFn rfn = fp64 ? pick_resume_batch_t<double>(gas, hasq) : pick_resume_batch_t<float>(gas, hasq);
-  int per_sm = 0, rper_sm = 0;
+  int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, BLOCK, 0));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, RBLOCK, 0));
   size_t grid = (size_t)std::max(per_sm, 1) * lead->sm_count;
   grid = std::min(grid, std::max<size_t>(1, (total + BLOCK - 1) / BLOCK));
   CK(cudaEventRecord(lead->ev[5], s));
   fn<<<(unsigned)grid, BLOCK, 0, s>>>(k, lead->d_kparams);
   CK(cudaGetLastError());
   CK(cudaEventRecord(lead->ev[6], s));
-  rfn<<<(unsigned)((size_t)std::max(rper_sm, 1) * lead->sm_count), RBLOCK, 0, s>>>(k, lead->d_kparams);
-  CK(cudaGetLastError());
+  rc = launch_warp_pass<true>(lead, rfn, RBLOCK, k, s);
+  if (rc) return rc;
   CK(cudaEventRecord(lead->ev[7], s));
   lead->last.grid_size = (int32_t)grid;
   lead->last.block_size = BLOCK;
@@ -665,7 +711,7 @@ int ccs_create(ccs_ctx **out, int device) {
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(CCS_ERR_CUDA);
   for (auto &e : c->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return bail(CCS_ERR_CUDA);
-  if (cudaMalloc(&c->d_work, 11 * sizeof(unsigned long long)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
+  if (cudaMalloc(&c->d_work, 13 * sizeof(unsigned long long)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
   if (cudaMalloc(&c->d_error, sizeof(int)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
   if (cudaMalloc(&c->d_kparams, sizeof(KParams)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
   *out = c;
@@ -680,6 +726,7 @@ void ccs_destroy(ccs_ctx *c) {
   dfree(c->d_vtab_v); dfree(c->d_vtab_s);
   dfree(c->d_work); dfree(c->d_error); dfree(c->d_rnd); dfree(c->d_kparams); dfree(c->d_park);
   dfree(c->d_bkp); dfree(c->d_bstart);
+  dfree(c->d_spec_rec); dfree(c->d_spec_out);
   dfree(c->d_key); dfree(c->d_key2); dfree(c->d_idx); dfree(c->d_idx2); dfree(c->d_sort_tmp);
   dfree(c->d_status); dfree(c->d_omc); dfree(c->d_steps); dfree(c->d_visits);
   for (auto &e : c->ev)

@@ -33,7 +33,7 @@ class CcsParams(ctypes.Structure):
         ("max_steps_per_try", ctypes.c_uint32),
         ("watchdog_s", ctypes.c_double),
         ("schedule", ctypes.c_int32), ("park_steps", ctypes.c_uint32),
-        ("resume_block", ctypes.c_int32),
+        ("resume_block", ctypes.c_int32), ("spec_tries", ctypes.c_int32),
     ]
 
 
@@ -44,7 +44,7 @@ class CcsStats(ctypes.Structure):
         ("steps", ctypes.c_uint64), ("visits", ctypes.c_uint64), ("parked", ctypes.c_uint64),
         ("kernel_ms", ctypes.c_double), ("h2d_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double),
         ("lanes_per_traj", ctypes.c_int32), ("block_size", ctypes.c_int32),
-        ("grid_size", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("grid_size", ctypes.c_int32), ("speculated", ctypes.c_int32),
         ("lane_ms", ctypes.c_double), ("warp_ms", ctypes.c_double),
     ]
 

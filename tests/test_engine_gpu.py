@@ -179,3 +179,21 @@ def test_co2_reference_velocity_quirk_matches_oracle(oracle):
     plain = engine_for(s, precision=1, quirks=0).run(s.predraw(400))
     sc = (plain["status"] == 1) & (out["status"] == 1)
     assert np.abs(plain["one_minus_cos"][sc] - out["one_minus_cos"][sc]).max() > 1e-3
+
+
+@pytest.mark.parametrize("prec", [1, 0])
+def test_speculative_tries_change_no_result(oracle, prec):
+    """A trajectory's tries run at once (speculatively) once it has failed two
+    in the warp pass; that changes the order of work, never a result: status,
+    1-cos(chi) and steps equal those of the sequential tries bit for bit."""
+    # few parked trajectories (speculation only runs when the warp pass is short of work)
+    s = oracle_system(oracle, target="c60.xyz", gas="He", ft=4, nprobe=20000)
+    rnd = s.predraw(20000)
+    seq = engine_for(s, precision=prec, lanes_per_traj=32, park_steps=1024, spec_tries=-1).run(rnd)
+    spec = engine_for(s, precision=prec, lanes_per_traj=32, park_steps=1024, spec_tries=2).run(rnd)
+    assert spec["stats"]["speculated"] > 0 and seq["stats"]["speculated"] == 0
+    assert np.array_equal(seq["status"], spec["status"])
+    assert np.array_equal(seq["steps"], spec["steps"])
+    assert np.array_equal(seq["one_minus_cos"], spec["one_minus_cos"])
+    for k in ("nfree", "nscatter", "nlost", "ncapped", "steps"):
+        assert seq["stats"][k] == spec["stats"][k], k
