@@ -426,7 +426,7 @@ def main():
     if rank == 0:
         status = st_pin
         nscatter = int((status == 1).sum())
-        m = n if args.fp64_check < 0 else args.fp64_check
+        m = (n if args.fp64_check < 0 else args.fp64_check) if world == 1 else 0  # N=1 line only
         accuracy = fp64_check(S, eng, pin_np, st_pin, om_pin, m, local) if m > 0 else None
         peak = E.measure_fp32_peak(local)
         engine_visits = last["visits"] / max(1, n)

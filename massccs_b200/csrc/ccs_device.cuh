@@ -865,11 +865,12 @@ template <typename T> __device__ __forceinline__ bool outside_box(const KParams 
 //             its own).  Probes out of reach feel exactly zero force.  A lane
 //             whose trajectory passes `park_steps` integration steps saves the
 //             exact integrator state to HBM ("parks" it) and takes new work.
-//  warp pass  parked trajectories resume one per warp: the force phase of a
-//             step uses all 32 lanes and the integrator runs warp-uniform, so
-//             the few very long trajectories (captured orbits with tens of
-//             thousands of steps) advance at the lowest per-step latency
-//             instead of sharing their warp with 31 others.
+//  warp pass  parked trajectories resume one per CTA (64 threads by
+//             default): the force phase of a step uses every thread and the
+//             integrator runs CTA-uniform, so the long trajectories (captured
+//             orbits with up to ~3e5 steps) advance at the lowest per-step
+//             latency instead of sharing a warp with 31 others; failed tries
+//             can run at once (speculative retries, see resume_kernel).
 //
 // Finished trajectories write status / 1-cos(chi) / steps / visits at their
 // own index.  Restarts rebuild the initial state from the trajectory's random
