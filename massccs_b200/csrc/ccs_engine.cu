@@ -310,6 +310,9 @@ KParams base_params(const ccs_ctx *c) {
 // Speculative-retry buffers for up to cap records (the park capacity) and
 // the counters d_work[11] (records) and d_work[12] (next speculative try).
 int setup_spec(ccs_ctx *c, KParams &k, size_t cap, cudaStream_t s) {
+  // records come only from warp passes with at most 2 parked trajectories per
+  // CTA slot (a few thousand); an overflow falls back to tries in sequence
+  cap = std::min<size_t>(cap, 65536);
   if (cap > c->spec_cap) {
     dfree(c->d_spec_rec); dfree(c->d_spec_out);
     c->spec_cap = 0;
@@ -431,7 +434,10 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   }
   // parking buffer for trajectories that outlast park_steps in the lane pass
   const size_t state_bytes = c->p.precision == CCS_PREC_FP64 ? sizeof(LaneState<double>) : sizeof(LaneState<float>);
-  const size_t cap = std::min<size_t>(n, std::max<size_t>(65536, n / 4));
+  // room for half the trajectories: a trajectory that finds the buffer full
+  // keeps running in its lane at the lane pass's per-step cost (measured: a
+  // park threshold that wanted 75,000+ slots of 75,000 tripled the run)
+  const size_t cap = std::min<size_t>(n, std::max<size_t>(65536, n / 2));
   if (cap * state_bytes > c->park_bytes) {
     dfree(c->d_park);
     c->park_bytes = 0;
@@ -593,7 +599,7 @@ int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const si
   k.deadline_ns = now + (unsigned long long)(wd * 1e9);
   const size_t state_bytes =
       lead->p.precision == CCS_PREC_FP64 ? sizeof(LaneState<double>) : sizeof(LaneState<float>);
-  const size_t cap = std::min<size_t>(total, std::max<size_t>(65536, total / 4));
+  const size_t cap = std::min<size_t>(total, std::max<size_t>(65536, total / 2));
   if (cap * state_bytes > lead->park_bytes) {
     dfree(lead->d_park);
     lead->park_bytes = 0;
