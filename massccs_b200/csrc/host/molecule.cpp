@@ -5,7 +5,10 @@
 // the per-gas Lennard-Jones pair parameters of the built-in tables or of a
 // user .ff file, moved to its centre of mass and rotated to its principal
 // axes with the longest extent on z -- the frame the trajectory loop uses.
+#include <charconv>
 #include <cmath>
+#include <cstring>
+#include <string_view>
 #include <fstream>
 #include <iostream>
 #include <sstream>
@@ -141,23 +144,91 @@ void resize_all(MoleculeTarget &t, int n) {
 }
 }  // namespace
 
+// Fast text input for multi-million-atom targets: the file is read whole and
+// split into lines and whitespace tokens in place; numbers go through
+// std::from_chars (correctly rounded, as the stream extraction the format
+// was defined with).  A line whose tokens are not plain numbers where numbers
+// are expected is parsed again with std::istringstream, so every input reads
+// exactly as with stream extraction.
+namespace {
+bool slurp(const std::string &path, std::string &buf) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return false;
+  f.seekg(0, std::ios::end);
+  const std::streamoff size = f.tellg();
+  if (size < 0) return false;
+  buf.resize((size_t)size);
+  f.seekg(0, std::ios::beg);
+  return size == 0 || (bool)f.read(&buf[0], size);
+}
+
+// std::getline's lines: split at '\n', the '\n' dropped, a last line kept
+// only if it holds characters
+struct Lines {
+  const char *p, *end;
+  bool next(std::string_view &line) {
+    if (p >= end) return false;
+    const char *q = static_cast<const char *>(std::memchr(p, '\n', (size_t)(end - p)));
+    const char *stop = q ? q : end;
+    line = std::string_view(p, (size_t)(stop - p));
+    p = q ? q + 1 : end;
+    return true;
+  }
+};
+
+inline bool space(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; }
+
+// the whitespace tokens of a line: up to maxt stored, all counted
+int tokens(std::string_view line, std::string_view *tok, int maxt) {
+  int n = 0;
+  size_t i = 0;
+  while (true) {
+    while (i < line.size() && space(line[i])) i++;
+    if (i >= line.size()) return n;
+    const size_t j = i;
+    while (i < line.size() && !space(line[i])) i++;
+    if (n < maxt) tok[n] = line.substr(j, i - j);
+    n++;
+  }
+}
+
+// a whole token that is a plain decimal number (what stream extraction reads
+// the same way); anything else returns false and the caller falls back
+bool plain_double(std::string_view t, double &v) {
+  if (!t.empty() && t[0] == '+') t.remove_prefix(1);
+  if (t.empty()) return false;
+  const char c = t[0];
+  if (!(c == '-' || c == '.' || (c >= '0' && c <= '9'))) return false;
+  if (c == '-' && (t.size() < 2 || !(t[1] == '.' || (t[1] >= '0' && t[1] <= '9')))) return false;
+  const auto r = std::from_chars(t.data(), t.data() + t.size(), v);
+  return r.ec == std::errc() && r.ptr == t.data() + t.size();
+}
+bool plain_long(std::string_view t, long &v) {
+  if (!t.empty() && t[0] == '+') t.remove_prefix(1);
+  if (t.empty() || t[0] == '+') return false;
+  const auto r = std::from_chars(t.data(), t.data() + t.size(), v);
+  return r.ec == std::errc() && r.ptr == t.data() + t.size();
+}
+}  // namespace
+
 // MoleculeTarget::readXYZfile (MoleculeTarget.cpp:148-319): atom count, a
 // comment line, then "Sym x y z" or "Sym x y z q" (charges dropped for force
 // types 1 and 2); every line must carry the same number of items.
 void MoleculeTarget::readXYZ(const std::string &path, int force_type) {
-  std::ifstream f(path);
-  std::string line;
+  std::string buf;
+  if (!slurp(path, buf)) throw std::invalid_argument("Error: missing number ot atoms in xyz file");
+  Lines L{buf.data(), buf.data() + buf.size()};
+  std::string_view line;
   int n = 0;
-  if (!f || !std::getline(f, line) || !(std::istringstream(line) >> n) || n < 0)
+  if (!L.next(line) || !(std::istringstream(std::string(line)) >> n) || n < 0)
     throw std::invalid_argument("Error: missing number ot atoms in xyz file");
-  std::getline(f, line);
-  std::vector<std::string> lines;
+  L.next(line);  // comment
+  std::vector<std::string_view> lines;
+  lines.reserve((size_t)n);
   int items0 = -1;
-  while (std::getline(f, line)) {
-    std::istringstream is(line);
-    std::string tok;
-    int items = 0;
-    while (is >> tok) items++;
+  std::string_view tok[5];
+  while (L.next(line)) {
+    const int items = tokens(line, tok, 5);
     if (items0 < 0) items0 = items;
     else if (items != items0) throw std::invalid_argument("Error: numbers of items by lines in the xyz file");
     lines.push_back(line);
@@ -167,11 +238,18 @@ void MoleculeTarget::readXYZ(const std::string &path, int force_type) {
   const bool charges = items0 != 4;
   resize_all(*this, n);
   for (int i = 0; i < n; i++) {
-    std::istringstream is(lines[i]);
     std::string sym;
     double xi = 0, yi = 0, zi = 0, qi = 0;
-    is >> sym >> xi >> yi >> zi;
-    if (charges) is >> qi;
+    const int nt = tokens(lines[i], tok, 5);
+    if (nt >= 4 && plain_double(tok[1], xi) && plain_double(tok[2], yi) && plain_double(tok[3], zi) &&
+        (!charges || (nt >= 5 && plain_double(tok[4], qi)))) {
+      sym = std::string(tok[0]);
+    } else {  // stream extraction, as the format defines it
+      xi = yi = zi = qi = 0;
+      std::istringstream is{std::string(lines[i])};
+      is >> sym >> xi >> yi >> zi;
+      if (charges) is >> qi;
+    }
     if (!charges || force_type == 1 || force_type == 2) qi = 0.0;
     name[i] = sym;
     assign(i, sym);
@@ -185,23 +263,29 @@ void MoleculeTarget::readXYZ(const std::string &path, int force_type) {
 // "ATOM serial name resName resSeq x y z q r"; the element is the first
 // letter of the atom name unless a user force field is given.
 void MoleculeTarget::readPQR(const std::string &path) {
-  std::ifstream f(path);
-  if (!f) throw std::invalid_argument("Error: reading pqr file " + path);
-  std::string line;
-  std::vector<std::string> atoms;
-  while (std::getline(f, line)) {
-    std::istringstream is(line);
-    std::string rec;
-    if (is >> rec && rec == "ATOM") atoms.push_back(line);
-  }
+  std::string buf;
+  if (!slurp(path, buf)) throw std::invalid_argument("Error: reading pqr file " + path);
+  Lines L{buf.data(), buf.data() + buf.size()};
+  std::string_view line;
+  std::vector<std::string_view> atoms;
+  std::string_view tok[9];
+  while (L.next(line))
+    if (tokens(line, tok, 1) > 0 && tok[0] == "ATOM") atoms.push_back(line);
   resize_all(*this, (int)atoms.size());
   for (int i = 0; i < natoms; i++) {
-    std::istringstream is(atoms[i]);
-    std::string rec, aname, res;
+    std::string aname;
     long serial, chain;
     double xi, yi, zi, qi;
-    if (!(is >> rec >> serial >> aname >> res >> chain >> xi >> yi >> zi >> qi))
-      throw std::invalid_argument("Error: unsupported PQR ATOM record: " + atoms[i]);
+    if (tokens(atoms[i], tok, 9) >= 9 && plain_long(tok[1], serial) && plain_long(tok[4], chain) &&
+        plain_double(tok[5], xi) && plain_double(tok[6], yi) && plain_double(tok[7], zi) &&
+        plain_double(tok[8], qi)) {
+      aname = std::string(tok[2]);
+    } else {  // stream extraction, as the format defines it
+      std::istringstream is{std::string(atoms[i])};
+      std::string rec, res;
+      if (!(is >> rec >> serial >> aname >> res >> chain >> xi >> yi >> zi >> qi))
+        throw std::invalid_argument("Error: unsupported PQR ATOM record: " + std::string(atoms[i]));
+    }
     const std::string sym = user_ff_flag_ ? aname : aname.substr(0, 1);
     name[i] = sym;
     assign(i, sym);

@@ -99,3 +99,21 @@ def test_synthetic_targets(host):
     G = host.System(synth.globule_n2(os.path.join(d, "glob"), nprobe=10, niter=1))
     assert G.info["natoms"] == 1231 and abs(G.info["target_charge"] - 4.0) < 1e-5
     assert G.info["force_type"] == 6 and G.info["gas_flag"] == 2
+
+
+def test_number_forms_read_as_stream_extraction(oracle, host):
+    """The whole-file reader (from_chars on plain numbers, stream extraction
+    for anything else) reads signs, exponents, bare fractions, CRLF line ends
+    and tabs exactly as the oracle's reader does."""
+    d = workdir()
+    lines = ["C +1.25 -0.5e1 .75 0.125", "C\t1.5E+01 -2 3. -0.25", "H 0.5 +2.5E-1 -1e0 +0.0625",
+             "O -3.75 4 0.0 0.0625", "N 2.5 -1.25 +3.5 0.0"]
+    with open(os.path.join(d, "forms.xyz"), "w", newline="") as f:
+        f.write("5\r\ncomment\r\n" + "\r\n".join(lines) + "\r\n")
+    with open(os.path.join(d, "forms_lf.xyz"), "w") as f:
+        f.write("5\ncomment\n" + "\n".join(lines) + "\n")
+    for name in ("forms.xyz", "forms_lf.xyz"):
+        p = write_input(d, input_dict(name, "He", 4, nprobe=10, niter=1), name=name + ".json")
+        S, O = host.System(p), oracle.OracleSystem(p)
+        np.testing.assert_array_equal(_sorted_target(S.target()), _sorted_target(O.target()))
+        assert S.info["target_charge"] == O.params["target_charge"]
