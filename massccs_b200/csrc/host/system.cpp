@@ -67,8 +67,6 @@ SystemSetup::SystemSetup(const std::string &json_path, bool print)
     : in(read_and_print(json_path, print)),
       gas(in.gas_buffer_flag),
       target(build_target(in, json_path, print, t_orient)) {
-  if (in.equipotential_flag == 1)
-    throw std::invalid_argument("Equipotential: yes is not supported by this engine; use the geometric ellipsoid");
   force_type = select_force_type(in);
   const int g = in.gas_buffer_flag;
   // reduced mass, molecular inertia (System.cpp:97-114)
@@ -88,38 +86,15 @@ SystemSetup::SystemSetup(const std::string &json_path, bool print)
   }
   alpha = in.alpha * 331.842254885;  // ALPHA_TO_KCAL_MOL (System.cpp:117)
 
-  // geometric ellipsoid (System.cpp:1640-1698): axes grown in 0.01 A steps
-  // until every atom pushed outward by radius + d lies inside
   double t0 = now_s();
-  const double mX = std::fabs(target.maxX), mY = std::fabs(target.maxY), mZ = std::fabs(target.maxZ);
-  const double d = gas.d;
-  const double radius = in.long_range_flag == 1 ? 2.0 * in.coul_cutoff : 2.0 * in.lj_cutoff;
-  if (print) {
-    std::cout << "*********************************************************" << std::endl;
-    std::cout << "Geometric Ellipsoid: " << std::endl;
-    std::cout << "*********************************************************" << std::endl;
-    std::cout << "maximal distances: " << mX << "  " << mY << "  " << mZ << "  Ang" << std::endl;
-  }
-  a = mX + radius + in.skin + d;
-  b = mY + radius + in.skin + d;
-  c = mZ + radius + in.skin + d;
-  if (print) std::cout << "Initial axis length: " << a << "  " << b << "  " << c << "  Ang" << std::endl;
-  for (int i = 0; i < target.natoms; i++) {
-    const double xi = target.x[i], yi = target.y[i], zi = target.z[i];
-    const double ri = std::sqrt(xi * xi + yi * yi + zi * zi);
-    const double px = xi + (radius + d) * (xi / ri), py = yi + (radius + d) * (yi / ri),
-                 pz = zi + (radius + d) * (zi / ri);
-    while (std::pow(px / a, 2) + std::pow(py / b, 2) + std::pow(pz / c, 2) > 1.0) {
-      a += 0.01;
-      b += 0.01;
-      c += 0.01;
-    }
+  if (in.equipotential_flag == 1) {  // System.cpp:120-126
+    equipotential_ellipsoid(target, g, in.polarizability_flag, in.temperatureTarget, mu, alpha, print, a, b, c);
+    if (print) std::cout << "ellipsoid axis length: " << a << "  " << b << "  " << c << "  Ang" << std::endl;
+  } else {
+    geometric_ellipsoid(print);
   }
   t_ellipsoid = now_s() - t0;
-  if (print) {
-    std::cout << "Ellipsoid axis length: " << a << "  " << b << "  " << c << "  Ang" << std::endl;
-    std::cout << "ellipsoid calculation time: " << t_ellipsoid << "s" << std::endl;
-  }
+  if (print) std::cout << "ellipsoid calculation time: " << t_ellipsoid << " s" << std::endl;
   bmax = std::fmax(std::fmax(a, b), c);
   if (print) std::cout << "maximal impact parameter: " << bmax << " Ang" << std::endl;
 
@@ -167,6 +142,37 @@ SystemSetup::SystemSetup(const std::string &json_path, bool print)
     std::cout << "lz: " << Lz << " Ang" << std::endl;
     std::cout << "linked-cell calculation time: " << t_cells << " s" << std::endl;
   }
+}
+
+// System::geometric_ellipsoid (System.cpp:1640-1698)
+void SystemSetup::geometric_ellipsoid(bool print) {
+  // geometric ellipsoid (System.cpp:1640-1698): axes grown in 0.01 A steps
+  // until every atom pushed outward by radius + d lies inside
+  const double mX = std::fabs(target.maxX), mY = std::fabs(target.maxY), mZ = std::fabs(target.maxZ);
+  const double d = gas.d;
+  const double radius = in.long_range_flag == 1 ? 2.0 * in.coul_cutoff : 2.0 * in.lj_cutoff;
+  if (print) {
+    std::cout << "*********************************************************" << std::endl;
+    std::cout << "Geometric Ellipsoid: " << std::endl;
+    std::cout << "*********************************************************" << std::endl;
+    std::cout << "maximal distances: " << mX << "  " << mY << "  " << mZ << "  Ang" << std::endl;
+  }
+  a = mX + radius + in.skin + d;
+  b = mY + radius + in.skin + d;
+  c = mZ + radius + in.skin + d;
+  if (print) std::cout << "Initial axis length: " << a << "  " << b << "  " << c << "  Ang" << std::endl;
+  for (int i = 0; i < target.natoms; i++) {
+    const double xi = target.x[i], yi = target.y[i], zi = target.z[i];
+    const double ri = std::sqrt(xi * xi + yi * yi + zi * zi);
+    const double px = xi + (radius + d) * (xi / ri), py = yi + (radius + d) * (yi / ri),
+                 pz = zi + (radius + d) * (zi / ri);
+    while (std::pow(px / a, 2) + std::pow(py / b, 2) + std::pow(pz / c, 2) > 1.0) {
+      a += 0.01;
+      b += 0.01;
+      c += 0.01;
+    }
+  }
+  if (print) std::cout << "Ellipsoid axis length: " << a << "  " << b << "  " << c << "  Ang" << std::endl;
 }
 
 void predraw(const SystemSetup &S, uint32_t seed, size_t n, double *rnd) {

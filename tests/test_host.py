@@ -117,3 +117,27 @@ def test_number_forms_read_as_stream_extraction(oracle, host):
         S, O = host.System(p), oracle.OracleSystem(p)
         np.testing.assert_array_equal(_sorted_target(S.target()), _sorted_target(O.target()))
         assert S.info["target_charge"] == O.params["target_charge"]
+
+
+REF_BIN = os.path.join(os.path.dirname(GOLDEN), os.pardir, "oracle", "_ref", "massccs")
+
+
+@pytest.mark.parametrize("target,gas,ft", [("c60.xyz", "He", 4), ("c60.xyz", "N2", 6), ("c60.xyz", "CO2", 4),
+                                            ("04_1ubq_charge_4e_min.pqr", "He", 4)])
+def test_equipotential_ellipsoid_matches_reference_binary(host, target, gas, ft):
+    """"Equipotential": "yes" (Equipotential.cpp): the host's axes against the
+    reference binary's report, which prints them to 6 significant digits."""
+    import re
+    import subprocess
+    if not os.access(REF_BIN, os.X_OK):
+        pytest.skip("reference binary not built here")
+    d = workdir()
+    cfg = dict(input_dict(target, gas, ft, nprobe=2, niter=1), Equipotential="yes", nthreads=4)
+    p = write_input(d, cfg)
+    out = subprocess.run([os.path.abspath(REF_BIN), "input.json"], cwd=d, capture_output=True, text=True,
+                         timeout=600).stdout
+    ref = [float(v) for v in re.search(r"^ellipsoid axis length: (\S+)\s+(\S+)\s+(\S+)", out, re.M).groups()]
+    S = host.System(p)
+    for k, r in zip("abc", ref):
+        assert abs(S.info[k] - r) <= 6e-6 * r, (k, S.info[k], r)
+    assert S.info["bmax"] == max(S.info["a"], S.info["b"], S.info["c"])
