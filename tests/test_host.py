@@ -122,7 +122,8 @@ def test_number_forms_read_as_stream_extraction(oracle, host):
 REF_BIN = os.path.join(os.path.dirname(GOLDEN), os.pardir, "oracle", "_ref", "massccs")
 
 
-@pytest.mark.parametrize("target,gas,ft", [("c60.xyz", "He", 4), ("c60.xyz", "N2", 6), ("c60.xyz", "CO2", 4),
+@pytest.mark.parametrize("target,gas,ft", [("c60.xyz", "He", 4), ("c60.xyz", "He", 2), ("c60.xyz", "N2", 6),
+                                            ("c60.xyz", "N2", 4), ("c60.xyz", "CO2", 4),
                                             ("04_1ubq_charge_4e_min.pqr", "He", 4)])
 def test_equipotential_ellipsoid_matches_reference_binary(host, target, gas, ft):
     """"Equipotential": "yes" (Equipotential.cpp): the host's axes against the
