@@ -101,6 +101,26 @@ def test_synthetic_targets(host):
     assert G.info["force_type"] == 6 and G.info["gas_flag"] == 2
 
 
+def test_batch_workload_generator(host):
+    """The batched-ion workload: log-uniform sizes in range, integer net
+    charges in [0, 30] e, the 1.0 A minimum distance, seeded (same files twice)."""
+    from scipy.spatial import cKDTree
+    from massccs_b200 import synth
+    d = workdir(())
+    paths = synth.batch(os.path.join(d, "b1"), nions=6, ntraj=10, nmin=500, nmax=5000)
+    again = synth.batch(os.path.join(d, "b2"), nions=6, ntraj=10, nmin=500, nmax=5000)
+    for p, q in zip(paths, again):
+        S = host.System(p)
+        assert 500 <= S.info["natoms"] <= 5000 and S.info["gas_flag"] == 1
+        Q = S.info["target_charge"]
+        assert abs(Q - round(Q)) < 1e-6 and 0 <= round(Q) <= 30
+        t = S.target()
+        xyz = np.stack([t["x"], t["y"], t["z"]], 1)
+        assert not cKDTree(xyz).query_pairs(1.0 - 1e-9)
+        a = open(os.path.join(os.path.dirname(p), "target.xyz")).read()
+        assert a == open(os.path.join(os.path.dirname(q), "target.xyz")).read()
+
+
 def test_number_forms_read_as_stream_extraction(oracle, host):
     """The whole-file reader (from_chars on plain numbers, stream extraction
     for anything else) reads signs, exponents, bare fractions, CRLF line ends
