@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <iostream>
 #include <random>
+#include <vector>
 
 #include "setup.h"
 
@@ -175,21 +176,66 @@ void SystemSetup::geometric_ellipsoid(bool print) {
   if (print) std::cout << "Ellipsoid axis length: " << a << "  " << b << "  " << c << "  Ang" << std::endl;
 }
 
+namespace {
+// MT19937 (Matsumoto and Nishimura, 1998), the generator the reference draws
+// from (std::mt19937 in RandomNumber.cpp:19-29), producing whole blocks of
+// 624 tempered words: the bulk form of the same sequence.  The twist is
+// split where its index wraps, so both halves and the tempering vectorise.
+constexpr int MT_N = 624, MT_M = 397;
+
+inline uint32_t mt_mix(uint32_t a, uint32_t b, uint32_t c) {
+  const uint32_t y = (a & 0x80000000u) | (b & 0x7fffffffu);
+  return c ^ (y >> 1) ^ ((0u - (y & 1u)) & 0x9908b0dfu);
+}
+
+__attribute__((target_clones("avx2", "default")))
+void mt_block(uint32_t *__restrict s, uint32_t *__restrict out) {
+  for (int i = 0; i < MT_N - MT_M; i++) s[i] = mt_mix(s[i], s[i + 1], s[i + MT_M]);
+  for (int i = MT_N - MT_M; i < MT_N - 1; i++) s[i] = mt_mix(s[i], s[i + 1], s[i + MT_M - MT_N]);
+  s[MT_N - 1] = mt_mix(s[MT_N - 1], s[0], s[MT_M - 1]);
+  for (int i = 0; i < MT_N; i++) {
+    uint32_t y = s[i];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    out[i] = y;
+  }
+}
+
+struct Mt19937Bulk {
+  static constexpr int N = MT_N;
+  uint32_t s[MT_N];
+  explicit Mt19937Bulk(uint32_t seed) {
+    s[0] = seed;
+    for (int i = 1; i < MT_N; i++) s[i] = 1812433253u * (s[i - 1] ^ (s[i - 1] >> 30)) + (uint32_t)i;
+  }
+  void block(uint32_t *out) { mt_block(s, out); }  // the next 624 outputs
+};
+}  // namespace
+
 void predraw(const SystemSetup &S, uint32_t seed, size_t n, double *rnd) {
-  // RandomNumber::getRandomNumber (RandomNumber.cpp:27-29): (r - min) / max, [0, 1]
-  std::mt19937 mt(seed);
-  const double mn = (double)std::mt19937::min(), mx = (double)std::mt19937::max();
-  auto u = [&]() { return ((double)mt() - mn) / mx; };
+  // System.cpp:185-197: per trajectory u1 (as sqrt(bmax^2 u1)), u2..u5, and
+  // u6..u9 for N2/CO2, in trajectory order; u = (r - min) / max
+  // (RandomNumber::getRandomNumber, RandomNumber.cpp:27-29).  The words are
+  // generated in bulk (the sequence is serial), then converted in parallel:
+  // the same divisions and square roots, so the same bits.
   const bool mol = S.in.gas_buffer_flag == 2 || S.in.gas_buffer_flag == 3;
-  for (size_t k = 5; k < 9; k++)
-    if (!mol)
-      for (size_t j = 0; j < n; j++) rnd[k * n + j] = 0.0;
+  const size_t K = mol ? 9 : 5;
+  const size_t total = K * n, blocks = (total + Mt19937Bulk::N - 1) / Mt19937Bulk::N;
+  std::vector<uint32_t> raw(blocks * Mt19937Bulk::N);
+  Mt19937Bulk mt(seed);
+  for (size_t b = 0; b < blocks; b++) mt.block(raw.data() + b * Mt19937Bulk::N);
+  const double mn = (double)std::mt19937::min(), mx = (double)std::mt19937::max();
   const double bmax2 = S.bmax * S.bmax;
-  for (size_t j = 0; j < n; j++) {  // System.cpp:185-197
-    rnd[j] = std::sqrt(bmax2 * u());
-    for (size_t k = 1; k < 5; k++) rnd[k * n + j] = u();
-    if (mol)
-      for (size_t k = 5; k < 9; k++) rnd[k * n + j] = u();
+#pragma omp parallel for schedule(static)
+  for (long long jj = 0; jj < (long long)n; jj++) {
+    const size_t j = (size_t)jj;
+    const uint32_t *r = raw.data() + j * K;
+    rnd[j] = std::sqrt(bmax2 * (((double)r[0] - mn) / mx));
+    for (size_t k = 1; k < K; k++) rnd[k * n + j] = ((double)r[k] - mn) / mx;
+    if (!mol)
+      for (size_t k = 5; k < 9; k++) rnd[k * n + j] = 0.0;
   }
 }
 

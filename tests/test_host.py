@@ -54,6 +54,17 @@ def test_setup_matches_oracle(oracle, host, target, gas, ft, ff):
 
 
 @pytest.mark.parametrize("gas", ["He", "N2"])
+def test_bulk_predraw_matches_oracle_on_a_long_odd_run(oracle, host, gas):
+    """The host draws the mt19937 words in blocks of 624 and converts them in
+    parallel; the rows must equal the oracle's one-by-one draws bit for bit
+    over many blocks and a count that ends inside a block."""
+    d = workdir()
+    p = write_input(d, input_dict("c60.xyz", gas, 4, nprobe=100003, niter=1))
+    S, O = host.System(p), oracle.OracleSystem(p)
+    np.testing.assert_array_equal(S.predraw(100003), O.predraw(100003))
+
+
+@pytest.mark.parametrize("gas", ["He", "N2"])
 def test_predraw_matches_oracle(oracle, host, gas):
     d = workdir()
     p = write_input(d, input_dict("c60.xyz", gas, 4, nprobe=300, niter=3))
