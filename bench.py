@@ -449,7 +449,8 @@ def main():
             "config": {"workload": args.config, "description": cfg["desc"], "trajectories_per_gpu": n,
                        "l2": "256 MiB buffer written between timed steps (outside the step events)",
                        "parallelism": f"{world} ranks, independent trajectory shards"},
-            "e2e": {"value": e2e_value, "unit": "trajectories/s", "h2d_bytes_per_step": 9 * 8 * n,
+            "e2e": {"value": e2e_value, "unit": "trajectories/s",
+                    "h2d_bytes_per_step": (9 if cfg["gas"] in ("N2", "CO2") else 5) * 8 * n,  # rows ccs_run copies
                     "d2h_bytes_per_step": 9 * n,
                     "includes": "host mt19937 pre-draw, H2D, lane+warp passes, D2H, reduction"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
