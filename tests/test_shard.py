@@ -71,3 +71,38 @@ def test_sharded_run_equals_single_process(oracle, world, tmp_path):
         np.testing.assert_array_equal(got["omega"], ref["omega"])
         np.testing.assert_array_equal(got["nfree"], ref["nfree"])
         assert float(got["ccs"]) == ref["ccs"] and float(got["err"]) == ref["err"]
+
+
+def _lost_rank_worker(rank, world, port, out_dir):
+    import datetime
+    import time
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=3))
+    from massccs_b200 import shard
+    if rank == 1:  # this rank fails before the gather: it never joins the collective
+        time.sleep(1.0)
+        open(os.path.join(out_dir, "rank1_left"), "w").close()
+        os._exit(0)
+    s, e = shard.shard_range(20, rank, world)
+    t0 = time.time()
+    try:
+        shard.sharded_ccs(np.ones(e - s, dtype=np.int8), np.zeros(e - s), 2, 10, 10.0)
+        result = "completed"
+    except Exception as exc:  # the surviving rank learns of the loss from the timeout
+        result = f"error after {time.time() - t0:.1f} s: {type(exc).__name__}"
+    open(os.path.join(out_dir, "rank0"), "w").write(result)
+    os._exit(0)
+
+
+def test_lost_rank_ends_the_gather_with_an_error(tmp_path):
+    """A rank that leaves before the final gather: the other rank's collective
+    ends with an error within the process group's timeout instead of waiting
+    forever (failure made on the host, CPU ranks)."""
+    import torch.multiprocessing as mp
+    mp.start_processes(_lost_rank_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    assert (tmp_path / "rank1_left").exists()
+    result = (tmp_path / "rank0").read_text()
+    assert result.startswith("error after"), result
+    assert float(result.split()[2]) < 60
