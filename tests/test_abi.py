@@ -64,3 +64,31 @@ def test_create_without_device_fails_cleanly(lib):
     h = ctypes.c_void_p()
     assert lib.ccs_create(ctypes.byref(h), 0) == -5  # CCS_ERR_NODEVICE
     assert not h.value
+
+
+def test_ctypes_layouts_match_the_headers(tmp_path):
+    """Every C struct of the ABI has the size and field offsets its ctypes
+    mirror assumes (compiled with the host C compiler against include/)."""
+    import shutil
+    import subprocess
+    from massccs_b200 import engine, host
+    cc = shutil.which("gcc") or "/usr/bin/gcc"
+    mirrors = {"ccs_params": engine.CcsParams, "ccs_stats": engine.CcsStats, "ccs_info": engine.CcsInfo,
+               "mh_info": host.MhInfo}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "massccs_gpu.h"', '#include "massccs_host.h"',
+             "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
