@@ -115,7 +115,7 @@ double norm3(const double p[3]) { return std::sqrt(p[0] * p[0] + p[1] * p[1] + p
 }  // namespace
 
 void equipotential_ellipsoid(const MoleculeTarget &t, int gas, int polarizability_flag, double temperature,
-                             double mu, double alpha, bool print, double &a, double &b, double &c) {
+                             double mu, double alpha, int nthreads, bool print, double &a, double &b, double &c) {
   const Probe U{t, gas, polarizability_flag != 0, alpha};
   // the energy threshold (Equipotential.cpp:31-37)
   const double v_mb = 2.0 * std::sqrt((2.0 * kB * temperature) / (M_PI * mu * kAmuKg));
@@ -147,7 +147,7 @@ void equipotential_ellipsoid(const MoleculeTarget &t, int gas, int polarizabilit
   // the points keep the reference's (level, rotation) order
   const int nrays = (levels + 1) * nrot;
   std::vector<std::array<double, 3>> hits((size_t)nrays, std::array<double, 3>{0.0, 0.0, 0.0});
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
   for (int ray = 0; ray < nrays; ray++) {
     const int i = ray / nrot, n = ray % nrot;
     const double zPos = -zMax + i * zInc;

@@ -92,7 +92,7 @@ struct SystemSetup {
 // the equipotential ellipsoid (Equipotential.cpp:19-715): a, b, c of the
 // surface where the probe's potential is 1 % of a slow particle's kinetic energy
 void equipotential_ellipsoid(const MoleculeTarget &t, int gas, int polarizability_flag, double temperature,
-                             double mu, double alpha, bool print, double &a, double &b, double &c);
+                             double mu, double alpha, int nthreads, bool print, double &a, double &b, double &c);
 
 int select_force_type(const Input &in);  // System.cpp:49-87
 std::string resolve_path(const std::string &json_path, const std::string &file);

@@ -1,5 +1,6 @@
 // system.cpp -- System::System up to the trajectory loop, the pre-draw and
 // the reduction (cces-cepid/massccs src/System.cpp:19-326, 1640-1698).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -89,7 +90,8 @@ SystemSetup::SystemSetup(const std::string &json_path, bool print)
 
   double t0 = now_s();
   if (in.equipotential_flag == 1) {  // System.cpp:120-126
-    equipotential_ellipsoid(target, g, in.polarizability_flag, in.temperatureTarget, mu, alpha, print, a, b, c);
+    equipotential_ellipsoid(target, g, in.polarizability_flag, in.temperatureTarget, mu, alpha,
+                            (int)std::max(1u, in.nthreads), print, a, b, c);
     if (print) std::cout << "ellipsoid axis length: " << a << "  " << b << "  " << c << "  Ang" << std::endl;
   } else {
     geometric_ellipsoid(print);
@@ -228,7 +230,7 @@ void predraw(const SystemSetup &S, uint32_t seed, size_t n, double *rnd) {
   for (size_t b = 0; b < blocks; b++) mt.block(raw.data() + b * Mt19937Bulk::N);
   const double mn = (double)std::mt19937::min(), mx = (double)std::mt19937::max();
   const double bmax2 = S.bmax * S.bmax;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads((int)std::max(1u, S.in.nthreads))
   for (long long jj = 0; jj < (long long)n; jj++) {
     const size_t j = (size_t)jj;
     const uint32_t *r = raw.data() + j * K;
