@@ -473,7 +473,6 @@ template <int GAS> struct RedShape {
 template <typename T, int G, int GAS>
 __device__ __forceinline__ void reduce_group_row(const Acc<T, GasShape<GAS>::NS> &acc, int g, unsigned mask,
                                                  T *row) {
-  constexpr int NS = GasShape<GAS>::NS;
   constexpr int NV = RedShape<GAS>::NV;
   if constexpr (G == 32) {
     constexpr int P = RedShape<GAS>::P;
