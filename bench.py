@@ -16,8 +16,10 @@ e2e        the same metric through the public host API (mh_predraw on the host,
 roofline   FP32-pipe roofline of the trajectory kernels: algorithmic flops (the
            reference's target-atom visits per trajectory x flops per visit) over
            the device time, against the device's measured FP32 FMA peak
-cpu_baseline  the reference binary (oracle/_ref/massccs) on this host's cores,
-           on a bounded sample of the same workload
+cpu_baseline  the reference binary (oracle/_ref/massccs[_v4], the highest ISA
+           level the host runs) on this host's cores, on a bounded sample of the
+           same workload (>= 3e4 trajectories), with the thread count (physical
+           cores or all logical CPUs) that runs it fastest
 accuracy   the metric's condition: the FP32 CCS against the engine's FP64
            mode on the same initial conditions (all of the step's trajectories
            by default; paired relative difference and its standard error)
@@ -37,7 +39,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "trajectories/s on 1 B200 at <=0.5% CCS err vs FP64: plain FP32 vs surrogate vs CPU"
-REF_BIN = os.path.join(ROOT, "oracle", "_ref", "massccs")
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+REF_SAMPLE = 30000  # fewest trajectories per timed reference sample
+
+
+def ref_sample_size(rs, total):
+    """Trajectories per timed reference sample: at least REF_SAMPLE and about
+    10 s of CPU work, at most the workload's own count."""
+    return int(min(total, max(REF_SAMPLE, rs["probe_rate"] * 10.0)) // 10 * 10)
 
 # flops per target-atom visit of one probe site (fixed constants of the work
 # model): LJ + induced dipole 45, LJ + Coulomb 25, Coulomb + induced dipole 40,
@@ -119,14 +128,49 @@ class ClockSampler:
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def ref_sample_run(json_path, nprobe, niter, threads):
+def host_cpu():
+    """CPU model, logical CPUs, physical cores and the AVX-512 subset the
+    x86-64-v4 build needs (from /proc/cpuinfo)."""
+    model, flags, cores, logical = None, set(), set(), 0
+    phys = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            k, _, v = line.partition(":")
+            k, v = k.strip(), v.strip()
+            if k == "processor":
+                logical += 1
+            elif k == "model name" and model is None:
+                model = v
+            elif k == "flags" and not flags:
+                flags = set(v.split())
+            elif k == "physical id":
+                phys = v
+            elif k == "core id":
+                cores.add((phys, v))
+    except OSError:
+        pass
+    logical = logical or (os.cpu_count() or 1)
+    v4 = {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= flags
+    return {"model": model, "logical_cpus": logical, "physical_cores": len(cores) or logical, "avx512": v4}
+
+
+def ref_binary(cpu):
+    """The reference binary at the highest ISA level this host supports."""
+    v4 = os.path.join(REF_DIR, "massccs_v4")
+    v3 = os.path.join(REF_DIR, "massccs")
+    if cpu["avx512"] and os.path.exists(v4):
+        return v4, "x86-64-v4"
+    return (v3, "x86-64-v3") if os.path.exists(v3) else (None, None)
+
+
+def ref_sample_run(binary, json_path, nprobe, niter, threads):
     """Run the reference binary on a sample; returns (trajectories, CCS time s, ccs)."""
     d = os.path.dirname(json_path)
     cfg = json.load(open(json_path))
     cfg.update({"numberProbe": nprobe, "nIter": niter, "nthreads": threads})
     p = os.path.join(d, "input_ref.json")
     json.dump(cfg, open(p, "w"))
-    out = subprocess.run([REF_BIN, "input_ref.json"], cwd=d, capture_output=True, text=True, timeout=1800)
+    out = subprocess.run([binary, "input_ref.json"], cwd=d, capture_output=True, text=True, timeout=1800)
     m = re.search(r"CCS time: (\S+) s", out.stdout)
     c = re.search(r"average value of CCS = (\S+)", out.stdout)
     if out.returncode != 0 or not m:
@@ -134,28 +178,49 @@ def ref_sample_run(json_path, nprobe, niter, threads):
     return nprobe * niter, float(m.group(1)), float(c.group(1)) if c else None
 
 
-def cpu_baseline(json_path, config):
-    """The reference binary on this host's cores, on a bounded sample, plus the
-    reference's visit count per trajectory (from the oracle, on a smaller
-    sample) for the roofline's algorithmic work."""
-    threads = os.cpu_count() or 1
-    out = {"value": None, "unit": "trajectories/s", "cores": threads, "kind": "reference", "sample": None}
-    visits = None
-    if os.path.exists(REF_BIN):
-        # about 10-30 s of CPU work: probe with a small run, then size the sample
-        n0, t0, _ = ref_sample_run(json_path, 200, 5, threads)
+def ref_setup(json_path):
+    """Binary, thread count and sample shape of the timed reference runs: the
+    faster of all physical cores and all logical CPUs on a probe sample of
+    2000 trajectories (the reference's results do not depend on it)."""
+    cpu = host_cpu()
+    binary, isa = ref_binary(cpu)
+    if binary is None:
+        return None
+    best = None
+    for threads in sorted({cpu["physical_cores"], cpu["logical_cpus"]}):
+        n0, t0, _ = ref_sample_run(binary, json_path, 200, 10, threads)
         rate = n0 / max(t0, 1e-3)
-        target = int(min(max(rate * 15.0, 2000), 200000))
+        if best is None or rate > best[1]:
+            best = (threads, rate)
+    return {"binary": binary, "isa": isa, "threads": best[0], "probe_rate": best[1], "cpu": cpu}
+
+
+def ref_describe(rs, n, nprobe, niter, extra=""):
+    c = rs["cpu"]
+    return (f"{n} trajectories ({nprobe} x {niter}) of the workload, reference binary "
+            f"{os.path.basename(rs['binary'])} ({rs['isa']}, -O3 -ffast-math, OpenMP), nthreads {rs['threads']} "
+            f"on {c['model']} ({c['physical_cores']} physical cores, {c['logical_cpus']} logical CPUs){extra}")
+
+
+def cpu_baseline(json_path, config):
+    """The reference binary on this host's cores, on a bounded sample of the
+    workload (REF_SAMPLE trajectories), plus the reference's visit count per
+    trajectory (from the oracle, on a smaller sample) for the roofline's
+    algorithmic work."""
+    out = {"value": None, "unit": "trajectories/s", "cores": None, "kind": "reference", "sample": None}
+    visits = None
+    rs = ref_setup(json_path)
+    if rs:
         niter = 10
-        nprobe = max(100, target // niter)
-        n, t, _ = ref_sample_run(json_path, nprobe, niter, threads)
-        out.update(value=n / t, sample=f"{n} trajectories ({nprobe} x {niter}) of the {config} workload, "
-                                           f"seed of the workload, nthreads {threads}; CCS time {t:.2f} s")
+        nprobe = ref_sample_size(rs, CONFIGS[config].get("ntraj", REF_SAMPLE)) // niter
+        n, t, _ = ref_sample_run(rs["binary"], json_path, nprobe, niter, rs["threads"])
+        out.update(value=n / t, cores=rs["threads"], isa=rs["isa"], cpu=rs["cpu"],
+                   sample=ref_describe(rs, n, nprobe, niter, f"; CCS time {t:.2f} s"))
     try:
         from oracle import pyoracle
         sys_ = pyoracle.OracleSystem(json_path)
         m = 400
-        res = sys_.run(sys_.predraw(m), nthreads=threads)
+        res = sys_.run(sys_.predraw(m), nthreads=os.cpu_count() or 1)
         visits = float(res["visits"].mean())
     except Exception as e:  # the roofline then reports the engine's own count only
         log("oracle visit count unavailable:", e)
@@ -191,29 +256,28 @@ def run_reference_arm(args, rank, world):
     line = {"metric": METRIC, "impl": "reference", "unit": "trajectories/s", "higher_is_better": True,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "dtype": "f64",
             "data": "synthetic", "config": {"workload": args.config, "description": cfg["desc"]}}
-    if not os.path.exists(REF_BIN):
+    if not os.path.exists(os.path.join(REF_DIR, "massccs")):
         line["unavailable"] = "reference binary oracle/_ref/massccs not built (make -C oracle ref)"
         print(json.dumps(line), flush=True)
         return
     d = tempfile.mkdtemp(prefix="bench_ref_")
     json_path = make_workload(args.config, d)
-    threads = os.cpu_count() or 1
-    n0, t0, _ = ref_sample_run(json_path, 200, 5, threads)
-    rate = n0 / max(t0, 1e-3)
-    per_step = int(min(max(rate * 8.0, 2000), 200000))  # ~8 s of CPU work per step
-    nprobe, niter = max(100, per_step // 10), 10
-    for _ in range(args.warmup):
-        ref_sample_run(json_path, max(100, nprobe // 10), niter, threads)
+    rs = ref_setup(json_path)
+    niter = 10
+    nprobe = ref_sample_size(rs, cfg.get("ntraj", REF_SAMPLE)) // niter  # >= 3e4 trajectories per timed step
+    for _ in range(args.warmup):  # warm-up steps at a tenth of the size
+        ref_sample_run(rs["binary"], json_path, nprobe // 10, niter, rs["threads"])
     times, n = [], 0
     for _ in range(args.steps):
-        k, t, _ = ref_sample_run(json_path, nprobe, niter, threads)
+        k, t, _ = ref_sample_run(rs["binary"], json_path, nprobe, niter, rs["threads"])
         times.append(t)
         n = k
     total = sum(times)
     value = n * len(times) / total
     line.update(value=value, ms_per_step=1e3 * total / len(times),
-                cpu_baseline={"value": value, "unit": "trajectories/s", "cores": threads, "kind": "reference",
-                              "sample": f"{n} trajectories per step ({nprobe} x {niter}), nthreads {threads}"},
+                cpu_baseline={"value": value, "unit": "trajectories/s", "cores": rs["threads"], "kind": "reference",
+                              "isa": rs["isa"], "cpu": rs["cpu"],
+                              "sample": ref_describe(rs, n, nprobe, niter, " per step; the reference's CCS time")},
                 e2e={"value": value, "unit": "trajectories/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
     shutil.rmtree(d, ignore_errors=True)
     print(json.dumps(line), flush=True)
@@ -460,7 +524,8 @@ def main():
                                   if ref_visits else "engine candidate visits per trajectory ") +
                                  f"{alg_visits:.4g} x {fpv:g} flops per visit",
                          "engine_visits_per_traj": engine_visits,
-                         "engine_tflops": n * engine_visits * fpv / kernel_s / 1e12},
+                         "engine_tflops": n * engine_visits * fpv / kernel_s / 1e12,
+                         "frac_executed": (n * engine_visits * fpv / kernel_s / 1e12) / peak if peak else None},
             "cpu_baseline": cpu,
             "accuracy": accuracy,
             "gpu_launches": 3 * args.steps,

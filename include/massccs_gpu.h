@@ -164,8 +164,12 @@ int ccs_run_batch(ccs_ctx *const *ions, size_t nions, const size_t *ntraj, const
                   ccs_stats *stats);
 
 /* Same on device buffers, asynchronous on `stream` (a cudaStream_t, NULL =
- * the context's stream).  d_rnd holds 9 rows of `stride` doubles.  Statistics
- * are accumulated on the device and read back by ccs_sync_stats. */
+ * the context's stream): the host does not wait for the GPU (the watchdog
+ * deadline is set on the device; the first run of a context with lanes_per_traj
+ * = 0 waits once for its autotuning).  d_rnd holds 9 rows of `stride` doubles.
+ * Statistics are accumulated on the device and read back by ccs_sync_stats,
+ * which waits for the run and returns CCS_ERR_TIMEOUT if the watchdog
+ * stopped it. */
 int ccs_run_device(ccs_ctx *ctx, size_t ntraj, const double *d_rnd, size_t stride,
                    int8_t *d_status, double *d_one_minus_cos, uint32_t *d_steps,
                    uint32_t *d_visits, void *stream);
@@ -176,10 +180,11 @@ int ccs_sync_stats(ccs_ctx *ctx, ccs_stats *stats);
  * cannot allocate device memory while they run -- a host whose allocator owns
  * the whole device heap, a service with a memory budget fixed at start-up, or
  * code where an allocation would synchronise the device.  The run's scratch
- * (work counter, statistics, launch-parameter copy, park buffer of long
- * trajectories) is a 24 MiB static device array that every GPU loading the
- * library holds until exit; inputs and outputs are the caller's device
- * buffers, as for ccs_run_device, and the results are the same.
+ * (work counter, statistics, watchdog deadline, launch-parameter copy, park
+ * buffer of long trajectories) is a 40 MiB static device array that every GPU
+ * loading the library holds until exit; inputs and outputs are the caller's
+ * device buffers, as for ccs_run_device, and the results are the same bit for
+ * bit (the park buffer has ccs_run_device's capacity at every allowed size).
  *  - at most 262144 trajectories per call (CCS_ERR_INVALID beyond that);
  *  - the first call on a device looks up the array's device address; make it
  *    before any stream capture;
@@ -188,7 +193,12 @@ int ccs_sync_stats(ccs_ctx *ctx, ccs_stats *stats);
  *    threads, other contexts on the same device) race, so serialise them;
  *  - lanes per force evaluation: the configured value, else the one the
  *    context already tuned, else 32 (no autotuning run);
- *  - stats may be NULL; when given, the call waits for the run and fills it. */
+ *  - stats == NULL: the call returns without waiting for the GPU; a later
+ *    ccs_sync_stats(ctx) waits for the run, fills the statistics from the
+ *    array and returns CCS_ERR_TIMEOUT if the watchdog stopped it (before
+ *    another call on the same device reuses the array);
+ *  - stats given: the call waits for the run, fills stats and returns
+ *    CCS_ERR_TIMEOUT if the watchdog stopped it. */
 int ccs_run_device_noalloc(ccs_ctx *ctx, size_t ntraj, const double *d_rnd, size_t stride,
                            int8_t *d_status, double *d_one_minus_cos, uint32_t *d_steps,
                            uint32_t *d_visits, void *stream, ccs_stats *stats);

@@ -66,7 +66,9 @@ struct KParams {
   double half_kconv_over_m1, half_kconv_over_m2, inv_m1, inv_m2, mu12, mu12_over_m1, mu12_over_m2;
   int quirks;
   uint32_t max_steps;
-  unsigned long long deadline_ns;
+  // watchdog: the %globaltimer value after which the kernels stop, written on
+  // the device by arm_watchdog just before the passes (no host round trip)
+  const unsigned long long *deadline;
   // speed sampler table (System.cpp:1537-1555)
   const double *vtab_v, *vtab_s;
   int vtab_n;
@@ -110,6 +112,12 @@ __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
+}
+
+// Sets the run's watchdog deadline to now + budget_ns (one thread, enqueued on
+// the run's stream before the trajectory passes).
+__global__ void arm_watchdog(unsigned long long *deadline, unsigned long long budget_ns) {
+  *deadline = global_ns() + budget_ns;
 }
 
 // A trajectory handed to the speculative phase: it failed try tries - 1 and
@@ -1207,6 +1215,8 @@ __global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParam
   LaneState<T> L;
   L.mode = M_IDLE;
   L.ion = 0;
+  const unsigned long long deadline = *(volatile const unsigned long long *)kp.deadline;
+  bool park_full = false;  // the park buffer filled up: stop asking for slots (it only fills)
 
   // take trajectories until one hits the ellipsoid (misses are written as free)
   auto grab = [&]() {
@@ -1245,7 +1255,7 @@ __global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParam
   for (;;) {
     if ((++it & 127u) == 0) {  // watchdog, one answer per warp
       int e = 0;
-      if (lane == 0) e = global_ns() > kp.deadline_ns || *(volatile int *)kp.error;
+      if (lane == 0) e = global_ns() > deadline || *(volatile int *)kp.error;
       e = __shfl_sync(FULL, e, 0);
       if (e) {
         if (lane == 0) atomicExch(kp.error, 1);
@@ -1350,12 +1360,14 @@ __global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParam
           load_init<T, GAS>(L, lane_setup<T, GAS>(ion_params_ptr<BATCH>(kp, kpg, L.ion), L.j));
           L.mode = M_RESTART;
         }
-      } else if (kp.park && L.nsteps >= kp.park_steps) {
+      } else if (kp.park && !park_full && L.nsteps >= kp.park_steps) {
         const unsigned long long slot = atomicAdd(kp.park_count, 1ull);
         if (slot < kp.park_cap) {
           reinterpret_cast<LaneState<T> *>(kp.park)[slot] = L;
           atomicAdd(&blk[7], 1ull);
           grab();
+        } else {
+          park_full = true;  // the trajectory stays in its lane
         }
       }
     }
@@ -1393,6 +1405,7 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
   __syncthreads();
   const int tid = threadIdx.x;
   const bool spec = kp.spec_phase != 0;
+  const unsigned long long deadline = *(volatile const unsigned long long *)kp.deadline;
   unsigned long long np;
   if (spec) {
     np = *(volatile unsigned long long *)kp.spec_count;
@@ -1441,7 +1454,7 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
       int r = S_CONTINUE;
       double omc = 0.0;
       if ((it & 1023u) == 0) {
-        if (tid == 0) sm_idx = (global_ns() > kp.deadline_ns || *(volatile int *)kp.error) ? 1ull : 0ull;
+        if (tid == 0) sm_idx = (global_ns() > deadline || *(volatile int *)kp.error) ? 1ull : 0ull;
         __syncthreads();
         const bool e = sm_idx != 0;
         __syncthreads();

@@ -79,6 +79,10 @@ struct ccs_ctx {
   // launch choice
   int tuned_G = 0, tuned_block = 0;
   ccs_stats last{};
+  // where the last run keeps its counters and error flag (the context's own
+  // buffers, or the static scratch of ccs_run_device_noalloc)
+  unsigned long long *run_work = nullptr;
+  int *run_error = nullptr;
 };
 
 namespace {
@@ -370,23 +374,16 @@ int ensure_run_buffers(ccs_ctx *c, size_t n, bool need_rnd) {
   return CCS_OK;
 }
 
-}  // namespace
-
-// ---------------------------------------------------------------------------
-// device clock helper: one-thread kernel reading %globaltimer
-__global__ void read_globaltimer(unsigned long long *out) { *out = global_ns(); }
-
-namespace {
-int device_now_ns(ccs_ctx *c, unsigned long long &t) {
-  read_globaltimer<<<1, 1, 0, c->stream>>>(c->d_work + 8);
+// The watchdog deadline of a run: now + watchdog_s, set on the device at the
+// head of the run (stream-ordered, so the host never waits for the clock).
+int arm_deadline(ccs_ctx *c, unsigned long long *word, cudaStream_t s) {
+  const double wd = c->p.watchdog_s > 0 ? c->p.watchdog_s : 600.0;
+  arm_watchdog<<<1, 1, 0, s>>>(word, (unsigned long long)(wd * 1e9));
   CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(&t, c->d_work + 8, sizeof t, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
   return CCS_OK;
 }
 
-// Full asynchronous run on device buffers (the kernel's only host sync is the
-// watchdog clock read at the start).
+// Full asynchronous run on device buffers (no host synchronisation).
 int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t *d_status,
                double *d_omc, uint32_t *d_steps, uint32_t *d_visits, cudaStream_t s, int G,
                int block) {
@@ -398,10 +395,7 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   k.omc = d_omc;
   k.steps = d_steps;
   k.visits = d_visits;
-  unsigned long long now = 0;
-  int rc = device_now_ns(c, now);
-  if (rc) return rc;
-  const double wd = c->p.watchdog_s > 0 ? c->p.watchdog_s : 600.0;
+  int rc = CCS_OK;
   KernelFn fn = pick_traj(c, G);
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, 0));
@@ -409,7 +403,7 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   size_t grid = (size_t)per_sm * c->sm_count;
   const size_t max_useful = (n + block - 1) / block;  // one trajectory per lane
   if (grid > max_useful) grid = std::max<size_t>(1, max_useful);
-  k.deadline_ns = now + (unsigned long long)(wd * 1e9);
+  k.deadline = c->d_work + 8;
   // longest-expected-first processing order (a radix sort of the length keys)
   if (n > 1 && c->p.schedule == 1) {
     if (n > c->order_cap) {
@@ -451,11 +445,15 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   k.park_next = c->d_work + 10;
   rc = setup_spec(c, k, cap, s);
   if (rc) return rc;
-  // d_work: [0] work counter, [1..7] statistics, [8] clock scratch, [9] parked, [10] resumed,
+  // d_work: [0] work counter, [1..7] statistics, [8] watchdog deadline, [9] parked, [10] resumed,
   // [11] speculative records, [12] next speculative try
   CK(cudaMemsetAsync(c->d_work, 0, 8 * sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(c->d_work + 9, 0, 2 * sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(c->d_error, 0, sizeof(int), s));
+  rc = arm_deadline(c, c->d_work + 8, s);
+  if (rc) return rc;
+  c->run_work = c->d_work;
+  c->run_error = c->d_error;
   c->h_kparams = k;
   CK(cudaMemcpyAsync(c->d_kparams, &c->h_kparams, sizeof(KParams), cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(c->ev[5], s));
@@ -473,8 +471,10 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
 }
 
 int read_stats(ccs_ctx *c, ccs_stats *st, size_t n) {
-  unsigned long long h[12];  // d_work[1..12]: statistics, clock, park and speculation counters
+  unsigned long long h[12];  // work[1..12]: statistics, deadline, park and speculation counters
   int herr = 0;
+  unsigned long long *work = c->run_work ? c->run_work : c->d_work;
+  int *error = c->run_error ? c->run_error : c->d_error;
   {
     float a = 0, b = 0;
     CK(cudaEventSynchronize(c->ev[7]));
@@ -483,13 +483,13 @@ int read_stats(ccs_ctx *c, ccs_stats *st, size_t n) {
     c->last.lane_ms = a;
     c->last.warp_ms = b;
   }
-  CK(cudaMemcpyAsync(h, c->d_work + 1, sizeof h, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(&herr, c->d_error, sizeof herr, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(h, work + 1, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&herr, error, sizeof herr, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->last.ntraj = n;
   c->last.nfree = h[0]; c->last.nscatter = h[1]; c->last.nlost = h[2]; c->last.ncapped = h[3];
   c->last.steps = h[4]; c->last.visits = h[5]; c->last.parked = h[6];
-  c->last.speculated = (int32_t)std::min<unsigned long long>(h[10], c->spec_cap);
+  c->last.speculated = work == c->d_work ? (int32_t)std::min<unsigned long long>(h[10], c->spec_cap) : 0;
   if (st) *st = c->last;
   if (herr) return fail(c, CCS_ERR_TIMEOUT, "device watchdog expired after %.0f s",
                         c->p.watchdog_s > 0 ? c->p.watchdog_s : 600.0);
@@ -585,6 +585,7 @@ int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const si
     CK(cudaMalloc(&lead->d_bstart, (nions + 1) * sizeof(unsigned long long)));
     lead->bkp_cap = nions;
   }
+  for (size_t i = 0; i < nions; i++) kv[i].deadline = lead->d_work + 8;
   CK(cudaMemcpy(lead->d_bkp, kv.data(), nions * sizeof(KParams), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(lead->d_bstart, st.data(), (nions + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice));
   KParams k = base_params(lead);
@@ -592,11 +593,8 @@ int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const si
   k.ions = lead->d_bkp;
   k.ion_start = lead->d_bstart;
   k.nions = (int)nions;
-  unsigned long long now = 0;
-  int rc = device_now_ns(lead, now);
-  if (rc) return rc;
-  const double wd = lead->p.watchdog_s > 0 ? lead->p.watchdog_s : 600.0;
-  k.deadline_ns = now + (unsigned long long)(wd * 1e9);
+  int rc = CCS_OK;
+  k.deadline = lead->d_work + 8;
   const size_t state_bytes =
       lead->p.precision == CCS_PREC_FP64 ? sizeof(LaneState<double>) : sizeof(LaneState<float>);
   const size_t cap = std::min<size_t>(total, std::max<size_t>(65536, total / 2));
@@ -616,6 +614,10 @@ int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const si
   CK(cudaMemsetAsync(lead->d_work, 0, 8 * sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(lead->d_work + 9, 0, 2 * sizeof(unsigned long long), s));
   CK(cudaMemsetAsync(lead->d_error, 0, sizeof(int), s));
+  rc = arm_deadline(lead, lead->d_work + 8, s);
+  if (rc) return rc;
+  lead->run_work = lead->d_work;
+  lead->run_error = lead->d_error;
   lead->h_kparams = k;
   CK(cudaMemcpyAsync(lead->d_kparams, &lead->h_kparams, sizeof(KParams), cudaMemcpyHostToDevice, s));
   const int gas = gas_kind(lead->p.gas);
@@ -1181,20 +1183,23 @@ const char *ccs_last_error(ccs_ctx *c) { return c ? c->err.c_str() : "no context
 // handed the whole device heap to its own pool allocator, a real-time or
 // embedded service whose memory budget is fixed at start-up, or code running
 // where a cudaMalloc would synchronise the device or fail.  For them the
-// scratch of the trajectory passes (work counter, statistics, the device copy
-// of the launch parameters and the park buffer of long trajectories) lives in
-// this file-scope array instead of per-context allocations.  Every GPU that
-// loads the library holds it until the process exits.
+// scratch of the trajectory passes (work counter, statistics, watchdog
+// deadline, the device copy of the launch parameters and the park buffer of
+// long trajectories) lives in this file-scope array instead of per-context
+// allocations.  Every GPU that loads the library holds it until the process
+// exits.
 namespace {
-constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(24) << 20;  // 24 MiB per device
-constexpr size_t NOALLOC_HEADER_BYTES = 256;                // counters and the error flag
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(40) << 20;  // 40 MiB per device
+constexpr size_t NOALLOC_HEADER_BYTES = 256;                // counters, deadline and the error flag
 constexpr size_t NOALLOC_PARAMS_BYTES = 4096;               // the launch-parameter copy
 constexpr size_t NOALLOC_MAX_TRAJ = size_t(1) << 18;        // 262144 trajectories per call
-constexpr size_t NOALLOC_PARK_CAP = 65536;                  // the park capacity ccs_run_device uses for them
+// park capacity: the rule of ccs_run_device, min(n, max(65536, n / 2)), at the largest n
+constexpr size_t NOALLOC_PARK_CAP = NOALLOC_MAX_TRAJ / 2;
 static_assert(sizeof(KParams) <= NOALLOC_PARAMS_BYTES, "launch parameters do not fit");
 static_assert(NOALLOC_HEADER_BYTES + NOALLOC_PARAMS_BYTES + NOALLOC_PARK_CAP * sizeof(LaneState<double>) <=
                   NOALLOC_SCRATCH_BYTES,
               "park buffer does not fit");
+static_assert(12 * sizeof(unsigned long long) + sizeof(int) <= NOALLOC_HEADER_BYTES, "header does not fit");
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
@@ -1246,8 +1251,9 @@ extern "C" int ccs_run_device_noalloc(ccs_ctx *c, size_t n, const double *d_rnd,
   unsigned char *base = noalloc_scratch(c->device, serr);
   if (!base) return fail(c, CCS_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(serr));
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-  unsigned long long *work = reinterpret_cast<unsigned long long *>(base);  // [0] counter [1..7] stats [8] clock [9..10] park
-  int *error = reinterpret_cast<int *>(base + 11 * sizeof(unsigned long long));
+  // header: [0] work counter [1..7] statistics [8] watchdog deadline [9] parked [10] resumed, then the error flag
+  unsigned long long *work = reinterpret_cast<unsigned long long *>(base);
+  int *error = reinterpret_cast<int *>(base + 12 * sizeof(unsigned long long));
   KParams *kparams = reinterpret_cast<KParams *>(base + NOALLOC_HEADER_BYTES);
   void *park = base + NOALLOC_HEADER_BYTES + NOALLOC_PARAMS_BYTES;
   // lanes per force evaluation: the configured or already tuned value (no autotuning here)
@@ -1265,20 +1271,16 @@ extern "C" int ccs_run_device_noalloc(ccs_ctx *c, size_t n, const double *d_rnd,
   k.work = work;
   k.stats = work + 1;
   k.error = error;
+  k.deadline = work + 8;
   k.park = park;
-  k.park_cap = std::min<size_t>(n, NOALLOC_PARK_CAP);
+  k.park_cap = std::min<size_t>(n, std::max<size_t>(65536, n / 2));
   k.park_steps = c->p.park_steps ? c->p.park_steps : 2048u;
   k.park_count = work + 9;
   k.park_next = work + 10;
   // everything that must start at zero: counters, statistics, park counters, error flag
   CK(cudaMemsetAsync(base, 0, NOALLOC_HEADER_BYTES, s));
-  read_globaltimer<<<1, 1, 0, s>>>(work + 8);
-  CK(cudaGetLastError());
-  unsigned long long now = 0;
-  CK(cudaMemcpyAsync(&now, work + 8, sizeof now, cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
-  const double wd = c->p.watchdog_s > 0 ? c->p.watchdog_s : 600.0;
-  k.deadline_ns = now + (unsigned long long)(wd * 1e9);
+  int rc = arm_deadline(c, work + 8, s);
+  if (rc) return rc;
   copy_params_kernel<<<1, 1, 0, s>>>(k, kparams);
   CK(cudaGetLastError());
   KernelFn fn = pick_traj(c, G);
@@ -1286,26 +1288,26 @@ extern "C" int ccs_run_device_noalloc(ccs_ctx *c, size_t n, const double *d_rnd,
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, 0));
   size_t grid = (size_t)std::max(per_sm, 1) * c->sm_count;
   grid = std::min(grid, std::max<size_t>(1, (n + block - 1) / block));
+  CK(cudaEventRecord(c->ev[2], s));
+  CK(cudaEventRecord(c->ev[5], s));
   fn<<<(unsigned)grid, block, 0, s>>>(k, kparams);
   CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[6], s));
   KernelFn rfn = pick_resume(c);
   int rper_sm = 0;
   const int rnt = resume_threads(c);
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, rnt, 0));
   rfn<<<(unsigned)((size_t)std::max(rper_sm, 1) * c->sm_count), rnt, 0, s>>>(k, kparams);
   CK(cudaGetLastError());
-  if (stats) {
-    unsigned long long h[7];
-    int herr = 0;
-    CK(cudaMemcpyAsync(h, work + 1, sizeof h, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(&herr, error, sizeof herr, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    std::memset(stats, 0, sizeof *stats);
-    stats->ntraj = n;
-    stats->nfree = h[0]; stats->nscatter = h[1]; stats->nlost = h[2]; stats->ncapped = h[3];
-    stats->steps = h[4]; stats->visits = h[5]; stats->parked = h[6];
-    stats->lanes_per_traj = G; stats->block_size = block; stats->grid_size = (int32_t)grid;
-    if (herr) return fail(c, CCS_ERR_TIMEOUT, "device watchdog expired");
-  }
+  CK(cudaEventRecord(c->ev[7], s));
+  CK(cudaEventRecord(c->ev[3], s));
+  // ccs_sync_stats reads this run's counters and error flag from the scratch
+  c->run_work = work;
+  c->run_error = error;
+  c->last.ntraj = n;
+  c->last.grid_size = (int32_t)grid;
+  c->last.block_size = block;
+  c->last.lanes_per_traj = G;
+  if (stats) return ccs_sync_stats(c, stats);
   return CCS_OK;
 }

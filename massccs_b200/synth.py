@@ -20,6 +20,11 @@ configurations the engine is measured on (sizes and distributions as stated):
              uniform integer in [0, 30] e, He, 2e4 trajectories each; the
              minimum distance is enforced by thinning a uniform sample with
              a k-d tree (fast_globule_atoms), not by sequential addition.
+  field_globule  the learned-field configuration: 20,000 atoms (radius
+             1.3 N^(1/3) sqrt(5/3) = 45.5 A, 1.0 A minimum spacing by k-d
+             tree thinning), same element mix, charges N(0, 0.3 e) shifted
+             to a net +12 e, default force field; N2 or CO2 (force type 6),
+             1e6 trajectories.
 
 Every generator writes `target.xyz` (5 columns: symbol x y z q), `uff.ff`
 when used and `input.json` into a directory and returns the json path.
@@ -240,3 +245,15 @@ def shell(d, natoms=500000, r_in=100.0, r_out=130.0, net=40.0, gas="He", nprobe=
     write_xyz(os.path.join(d, "target.xyz"), _elements(natoms, rng), xyz, _charges(natoms, net, rng))
     ft = 6 if gas in ("N2", "CO2") else 4
     return write_input(d, "target.xyz", gas, ft, nprobe, niter, seed, extra=extra or None)
+
+
+def field_globule(d, gas="N2", natoms=20000, net=12.0, nprobe=100000, niter=10, seed=2104, gen_seed=20000,
+                  **extra):
+    """The learned-field workload: a 20,000-atom globule at +12 e with the N2
+    or CO2 probe, all force terms on (force type 6)."""
+    os.makedirs(d, exist_ok=True)
+    rng = np.random.default_rng(gen_seed)
+    radius = 1.3 * natoms ** (1 / 3) * (5 / 3) ** 0.5
+    sym, xyz, q = fast_globule_atoms(natoms, radius, net, rng)
+    write_xyz(os.path.join(d, "target.xyz"), sym, xyz, q)
+    return write_input(d, "target.xyz", gas, 6, nprobe, niter, seed, extra=extra or None)

@@ -20,7 +20,7 @@ import subprocess
 import sys
 import tempfile
 
-REF = "/root/reference"
+REF = os.environ.get("REFERENCE_DIR", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 REFBIN = os.path.join(ROOT, "oracle", "_ref", "massccs")

@@ -33,7 +33,12 @@ def _points(sys_, n, rng, near=True):
 CASES = [("c60.xyz", "He", 4), ("c60.xyz", "He", 2), ("c60.xyz", "He", 1), ("c60.xyz", "Ar", 4),
          ("04_1ubq_charge_4e_min.pqr", "He", 4), ("04_1ubq_charge_4e_min.pqr", "N2", 6),
          ("04_1ubq_charge_4e_min.pqr", "N2", 4), ("04_1ubq_charge_4e_min.pqr", "N2", 3),
-         ("04_1ubq_charge_4e_min.pqr", "CO2", 6), ("c60.xyz", "CO2", 4), ("c60.xyz", "co2", 2)]
+         ("04_1ubq_charge_4e_min.pqr", "CO2", 6), ("c60.xyz", "CO2", 4), ("c60.xyz", "co2", 2),
+         # all-pairs routines (force types 1/3/5: no cutoffs, no shifts; Force.cpp:117-300, 495-574,
+         # 836-897, 1169-1219, 1352-1415, 1637-1725)
+         ("c60.xyz", "He", 3), ("04_1ubq_charge_4e_min.pqr", "He", 3), ("04_1ubq_charge_4e_min.pqr", "N2", 5),
+         ("c60.xyz", "N2", 1), ("04_1ubq_charge_4e_min.pqr", "CO2", 5), ("c60.xyz", "CO2", 3),
+         ("c60.xyz", "CO2", 1)]
 
 
 @pytest.mark.parametrize("target,gas,ft", CASES)
@@ -90,7 +95,8 @@ def _paired(oracle, target, gas, ft, n, prec, quirks=0, **kw):
 
 TRAJ = [("c60.xyz", "He", 4, 3000), ("c60.xyz", "Ar", 4, 2000),
         ("04_1ubq_charge_4e_min.pqr", "He", 4, 1500), ("c60.xyz", "N2", 6, 1000),
-        ("04_1ubq_charge_4e_min.pqr", "N2", 6, 600), ("c60.xyz", "CO2", 4, 800)]
+        ("04_1ubq_charge_4e_min.pqr", "N2", 6, 600), ("c60.xyz", "CO2", 4, 800),
+        ("c60.xyz", "He", 3, 1500), ("c60.xyz", "N2", 5, 400), ("c60.xyz", "CO2", 5, 300)]
 
 
 @pytest.mark.parametrize("target,gas,ft,n", TRAJ)
