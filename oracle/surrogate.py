@@ -1,129 +1,227 @@
 """TEST INFRASTRUCTURE ONLY (the checker, never the product).
 
-A numpy restatement of the learned field the engine's fifth configuration
-calls for: a multiresolution hash-grid encoding of the probe position (the
-published Instant-NGP encoding: per level a grid of resolution
-base * growth**l, the 8 corners of the cell around the point looked up
-directly on coarse levels and through the spatial hash
-(x * 1) ^ (y * 2654435761) ^ (z * 805459861) mod T on fine ones, features
-interpolated trilinearly) feeding a ReLU MLP whose outputs are the site
-potentials.  Forces are minus the gradient of the potential with respect to
-the position, through the MLP and the interpolation weights.
+A numpy FP64 restatement of the learned field the engine trains and runs on
+the GPU (massccs_b200/csrc/field_device.cuh, field.cu).  The reference has
+no learned field, so no reference file restates this; the model is the
+published multiresolution hash encoding (Mueller et al., Instant-NGP, 2022)
+feeding a two-hidden-layer ReLU MLP:
 
-It gives the CUDA training and inference kernels their reference: the
-forward pass, the parameter gradients of a squared loss (hash-table
-gradients scatter-added), and the position gradient, all in FP64.  No
-reference file restates this: the reference has no learned field.
+  encoding   per level l: a grid of resolution res_l = floor(base * g**l),
+             g = (finest / base) ** (1 / (L - 1)), over the box [lo, hi];
+             the 8 corners of the cell around x read a table of T rows of F
+             features -- directly (x + r (y + r z), r = res_l + 1) while
+             r**3 <= T, else through the spatial hash
+             (x * 1) ^ (y * 2654435761) ^ (z * 805459861) mod T -- and are
+             blended with smoothstep weights S(f) = f^2 (3 - 2 f) per axis
+             (continuous first derivatives, so the forces of the field are
+             continuous).  e(x): L * F features; J(x) = de/dx.
+  MLP        z1 = W1 e + b1, a1 = relu(z1); z2 = W2 a1 + b2, a2 = relu(z2);
+             u_f = s (w3_f . a2 + b3_f) for each output field f (one per gas
+             site type), s a fixed output scale.
+  forces     F_f = -du_f/dx = -s J^T W1^T (m1 * W2^T (m2 * w3_f)), m = z > 0.
+  loss       per sample, sum over fields of
+               lam_u (u_f - U*_f)^2 / (U*_f^2 + u0^2) + |F_f - F*_f|^2 / (|F*_f|^2 + f0^2)
+             (relative errors with floors), averaged over the batch.  Its
+             parameter gradients pass twice through the network (the force
+             is itself a gradient): `loss_and_grad`.
+  inference  `infer_bf16`: the arithmetic of the tensor-core path -- table
+             and W1/W2 in bfloat16, the MMA inputs (features, hidden
+             activations, back-propagated vectors) rounded to bfloat16,
+             FP32-exact products summed in FP64 here.
+
+Weights are stored [out][in] (row-major), as on the GPU.
 """
 import numpy as np
 
 PRIMES = (1, 2654435761, 805459861)
 
 
+def bf16(a):
+    """Round to bfloat16 (nearest even) and back to float64."""
+    a = np.asarray(a, dtype=np.float32)
+    b = a.view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    return b.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
 class HashGrid:
-    def __init__(self, lo, hi, levels=16, log2_table=18, features=2, base=16, finest=2048, seed=0):
+    def __init__(self, lo, hi, levels=16, log2_table=18, features=2, base=16, finest=2048, seed=0,
+                 init=1e-4):
         self.lo = np.asarray(lo, dtype=np.float64)
         self.hi = np.asarray(hi, dtype=np.float64)
         self.L, self.T, self.F = levels, 1 << log2_table, features
         growth = np.exp((np.log(finest) - np.log(base)) / max(1, levels - 1))
         self.res = np.floor(base * growth ** np.arange(levels)).astype(np.int64)
         rng = np.random.default_rng(seed)
-        self.table = rng.uniform(-1e-4, 1e-4, size=(levels, self.T, features))
+        self.table = rng.uniform(-init, init, size=(levels, self.T, features))
+
+    def dense(self, level):
+        r = int(self.res[level]) + 1
+        return r ** 3 <= self.T
 
     def _index(self, level, c):
-        """Table rows of integer corners c (n, 3) on a level: direct on coarse levels."""
+        """Table rows of integer corners c (n, 3) on a level."""
         r = self.res[level] + 1
-        if r ** 3 <= self.T:
-            return (c[:, 0] + r * (c[:, 1] + r * c[:, 2])) % self.T
+        if self.dense(level):
+            return c[:, 0] + r * (c[:, 1] + r * c[:, 2])
         h = (c[:, 0].astype(np.uint64) * np.uint64(PRIMES[0])) ^ \
             (c[:, 1].astype(np.uint64) * np.uint64(PRIMES[1])) ^ \
             (c[:, 2].astype(np.uint64) * np.uint64(PRIMES[2]))
-        return (h % np.uint64(self.T)).astype(np.int64)
+        return ((h & np.uint64(0xFFFFFFFF)) % np.uint64(self.T)).astype(np.int64)
 
-    def _cells(self, x, level):
-        u = (x - self.lo) / (self.hi - self.lo)          # unit cube
-        p = np.clip(u, 0.0, 1.0) * self.res[level]
+    def corners(self, x, level):
+        """Per corner: rows (n, 8), weights (n, 8), weight gradients (n, 8, 3)."""
+        scale = self.res[level] / (self.hi - self.lo)          # grid units per A
+        p = np.clip((x - self.lo) * scale, 0.0, self.res[level])
         c0 = np.minimum(np.floor(p).astype(np.int64), self.res[level] - 1)
-        return p - c0, c0, self.res[level] / (self.hi - self.lo)  # fraction, corner, d(p)/d(x)
+        f = p - c0
+        S = f * f * (3.0 - 2.0 * f)
+        dS = 6.0 * f * (1.0 - f) * scale
+        rows, wts, dws = [], [], []
+        for corner in range(8):
+            o = np.array([(corner >> k) & 1 for k in range(3)])
+            w3 = np.where(o == 1, S, 1.0 - S)
+            d3 = np.where(o == 1, dS, -dS)
+            rows.append(self._index(level, c0 + o))
+            wts.append(w3.prod(axis=1))
+            dws.append(np.stack([d3[:, 0] * w3[:, 1] * w3[:, 2], w3[:, 0] * d3[:, 1] * w3[:, 2],
+                                 w3[:, 0] * w3[:, 1] * d3[:, 2]], axis=1))
+        return np.stack(rows, 1), np.stack(wts, 1), np.stack(dws, 1)
 
-    def encode(self, x, want_grad=False):
-        """x (n, 3) -> features (n, L*F); with want_grad also d(features)/dx (n, L*F, 3)
-        and the corner rows and weights for the backward pass."""
+    def encode(self, x, table=None):
+        """x (n, 3) -> e (n, L*F), J (n, L*F, 3), per-level corner caches."""
+        t = self.table if table is None else table
         x = np.atleast_2d(np.asarray(x, dtype=np.float64))
         n = x.shape[0]
-        out = np.zeros((n, self.L * self.F))
-        dout = np.zeros((n, self.L * self.F, 3)) if want_grad else None
+        e = np.zeros((n, self.L * self.F))
+        J = np.zeros((n, self.L * self.F, 3))
         cache = []
         for l in range(self.L):
-            f, c0, dpdx = self._cells(x, l)
-            rows, weights = [], []
-            for corner in range(8):
-                o = np.array([(corner >> k) & 1 for k in range(3)])
-                w3 = np.where(o == 1, f, 1.0 - f)          # per-axis weights (n, 3)
-                w = w3.prod(axis=1)
-                idx = self._index(l, c0 + o)
-                val = self.table[l, idx]                  # (n, F)
-                out[:, l * self.F:(l + 1) * self.F] += w[:, None] * val
-                if want_grad:
-                    for a in range(3):
-                        dw = np.where(o[a] == 1, 1.0, -1.0) * np.prod(np.delete(w3, a, axis=1), axis=1)
-                        dout[:, l * self.F:(l + 1) * self.F, a] += (dw * dpdx[a])[:, None] * val
-                rows.append(idx)
-                weights.append(w)
-            cache.append((np.stack(rows, 1), np.stack(weights, 1)))
-        return out, dout, cache
+            rows, w, dw = self.corners(x, l)
+            val = t[l][rows]                                   # (n, 8, F)
+            e[:, l * self.F:(l + 1) * self.F] = np.einsum("nc,ncf->nf", w, val)
+            J[:, l * self.F:(l + 1) * self.F, :] = np.einsum("nca,ncf->nfa", dw, val)
+            cache.append((rows, w, dw))
+        return e, J, cache
 
 
 class Field:
-    """Hash-grid encoding + MLP (ReLU hidden layers, linear output)."""
+    """Hash-grid encoding + MLP with one potential output per field."""
 
-    def __init__(self, lo, hi, hidden=(64, 64), outputs=1, seed=0, **grid):
+    def __init__(self, lo, hi, hidden=64, outputs=2, scale=1.0, seed=0, **grid):
         self.grid = HashGrid(lo, hi, seed=seed, **grid)
         rng = np.random.default_rng(seed + 1)
-        dims = [self.grid.L * self.grid.F, *hidden, outputs]
-        self.W = [rng.normal(0, np.sqrt(2.0 / a), size=(a, b)) for a, b in zip(dims[:-1], dims[1:])]
-        self.b = [np.zeros(b) for b in dims[1:]]
+        E = self.grid.L * self.grid.F
+        self.W1 = rng.normal(0, np.sqrt(2.0 / E), size=(hidden, E))
+        self.b1 = np.zeros(hidden)
+        self.W2 = rng.normal(0, np.sqrt(2.0 / hidden), size=(hidden, hidden))
+        self.b2 = np.zeros(hidden)
+        self.W3 = rng.normal(0, np.sqrt(1.0 / hidden), size=(outputs, hidden))
+        self.b3 = np.zeros(outputs)
+        self.s = float(scale)
+
+    # parameters as a flat MLP vector in the GPU's order: W1, b1, W2, b2, W3, b3
+    def mlp_vector(self):
+        return np.concatenate([self.W1.ravel(), self.b1, self.W2.ravel(), self.b2, self.W3.ravel(), self.b3])
+
+    def set_mlp_vector(self, v):
+        H, E = self.W1.shape
+        nf = self.W3.shape[0]
+        k = 0
+        for name, shape in (("W1", (H, E)), ("b1", (H,)), ("W2", (H, H)), ("b2", (H,)), ("W3", (nf, H)),
+                            ("b3", (nf,))):
+            m = int(np.prod(shape))
+            setattr(self, name, np.array(v[k:k + m], dtype=np.float64).reshape(shape))
+            k += m
 
     def forward(self, x):
-        h, dh, cache = self.grid.encode(x, want_grad=True)
-        acts, pre = [h], []
-        for k, (W, b) in enumerate(zip(self.W, self.b)):
-            z = acts[-1] @ W + b
-            pre.append(z)
-            acts.append(np.maximum(z, 0.0) if k < len(self.W) - 1 else z)
-        self._state = (dh, cache, acts, pre)
-        return acts[-1]
+        """u (n, nf), F (n, nf, 3) and the intermediate state."""
+        e, J, cache = self.grid.encode(x)
+        z1 = e @ self.W1.T + self.b1
+        m1 = z1 > 0
+        a1 = np.where(m1, z1, 0.0)
+        z2 = a1 @ self.W2.T + self.b2
+        m2 = z2 > 0
+        a2 = np.where(m2, z2, 0.0)
+        u = self.s * (a2 @ self.W3.T + self.b3)
+        g2 = m2[:, None, :] * self.W3[None, :, :]              # (n, nf, H)
+        g1 = m1[:, None, :] * (g2 @ self.W2)                   # (n, nf, H): W2^T g2
+        g0 = g1 @ self.W1                                      # (n, nf, E): W1^T g1
+        F = -self.s * np.einsum("nfe,nea->nfa", g0, J)
+        st = dict(e=e, J=J, cache=cache, z1=z1, m1=m1, a1=a1, z2=z2, m2=m2, a2=a2, g2=g2, g1=g1, g0=g0)
+        return u, F, st
 
-    def backward(self, dy):
-        """Gradients of sum(dy * y) for the weights, biases and hash table."""
-        dh, cache, acts, pre = self._state
-        gW, gb = [None] * len(self.W), [None] * len(self.b)
-        g = dy
-        for k in range(len(self.W) - 1, -1, -1):
-            if k < len(self.W) - 1:
-                g = g * (pre[k] > 0)
-            gW[k] = acts[k].T @ g
-            gb[k] = g.sum(axis=0)
-            g = g @ self.W[k].T
-        gt = np.zeros_like(self.grid.table)
-        F = self.grid.F
-        for l, (rows, weights) in enumerate(cache):
-            gl = g[:, l * F:(l + 1) * F]
-            for corner in range(8):
-                np.add.at(gt[l], rows[:, corner], weights[:, corner][:, None] * gl)
-        return gW, gb, gt, g
+    def loss_and_grad(self, x, U, Fs, lam_u=0.1, u0=0.05, f0=0.05):
+        """Mean loss over the batch and its gradients: (loss, dtable, dmlp vector).
+        U (n, nf), Fs (n, nf, 3) are the labels."""
+        n = x.shape[0]
+        u, F, st = self.forward(x)
+        wu = lam_u / (U * U + u0 * u0)                         # (n, nf)
+        wf = 1.0 / ((Fs * Fs).sum(-1) + f0 * f0)               # (n, nf)
+        du = u - U
+        dF = F - Fs
+        loss = float((wu * du * du + wf * (dF * dF).sum(-1)).sum() / n)
+        s = self.s
+        e, J, m1, a1, m2, a2, g2, g1, g0 = (st[k] for k in ("e", "J", "m1", "a1", "m2", "a2", "g2", "g1", "g0"))
+        du_ = 2.0 * wu * du / n                                # dL/du (n, nf)
+        eF = 2.0 * wf[..., None] * dF / n                      # dL/dF (n, nf, 3)
+        # ---- potential path
+        dW3 = s * du_.T @ a2
+        db3 = s * du_.sum(0)
+        da2 = s * du_ @ self.W3                                # (n, H)
+        dz2 = m2 * da2
+        dW2 = dz2.T @ a1
+        db2 = dz2.sum(0)
+        dz1 = m1 * (dz2 @ self.W2)
+        dW1 = dz1.T @ e
+        db1 = dz1.sum(0)
+        de = dz1 @ self.W1                                     # (n, E)
+        # ---- force path: F_f = -s J^T g0_f
+        r0 = -s * np.einsum("nea,nfa->nfe", J, eF)             # dL/dg0 (n, nf, E)
+        dJ = -s * np.einsum("nfe,nfa->nea", g0, eF)            # dL/dJ (n, E, 3)
+        dW1 += np.einsum("nfh,nfe->he", g1, r0)                # g0 = W1^T g1
+        r1 = r0 @ self.W1.T                                    # dL/dg1 (n, nf, H)
+        h = m1[:, None, :] * r1                                # through g1 = m1 * (W2^T g2)
+        dW2 += np.einsum("nfo,nfi->oi", g2, h)
+        r2 = h @ self.W2.T                                     # dL/dg2 (n, nf, H)
+        dW3 += np.einsum("nh,nfh->fh", m2, r2)                 # g2 = m2 * w3_f
+        # ---- table: e = sum_c w_c T[c], J = sum_c dw_c T[c]
+        dt = np.zeros_like(self.grid.table)
+        Fd = self.grid.F
+        for l, (rows, w, dw) in enumerate(st["cache"]):
+            ge = de[:, l * Fd:(l + 1) * Fd]                    # (n, F)
+            gJ = dJ[:, l * Fd:(l + 1) * Fd, :]                 # (n, F, 3)
+            contrib = w[:, :, None] * ge[:, None, :] + np.einsum("nca,nfa->ncf", dw, gJ)
+            np.add.at(dt[l], rows.ravel(), contrib.reshape(-1, Fd))
+        dmlp = np.concatenate([dW1.ravel(), db1, dW2.ravel(), db2, dW3.ravel(), db3])
+        return loss, dt, dmlp
 
-    def position_grad(self, x):
-        """d y / d x (n, outputs, 3): the force is minus this for a potential output."""
-        y = self.forward(x)
-        dh, cache, acts, pre = self._state
-        out = np.zeros((y.shape[0], y.shape[1], 3))
-        for j in range(y.shape[1]):
-            g = np.zeros_like(y)
-            g[:, j] = 1.0
-            for k in range(len(self.W) - 1, -1, -1):
-                if k < len(self.W) - 1:
-                    g = g * (pre[k] > 0)
-                g = g @ self.W[k].T
-            out[:, j, :] = np.einsum("nf,nfa->na", g, dh)
-        return out
+    def infer_bf16(self, x):
+        """u (n, nf), F (n, nf, 3) in the tensor-core inference arithmetic."""
+        e, J, _ = self.grid.encode(x, table=bf16(self.grid.table))
+        W1, W2 = bf16(self.W1), bf16(self.W2)
+        W3 = self.W3.astype(np.float32).astype(np.float64)
+        A1 = bf16(e)
+        z1 = A1 @ W1.T + self.b1
+        m1 = z1 > 0
+        A2 = bf16(np.where(m1, z1, 0.0))
+        z2 = A2 @ W2.T + self.b2
+        m2 = z2 > 0
+        a2 = np.where(m2, z2, 0.0)
+        u = self.s * (a2 @ W3.T + self.b3)
+        G2 = bf16(m2[:, None, :] * W3[None, :, :])
+        G1 = bf16(m1[:, None, :] * (G2 @ W2))
+        g0 = G1 @ W1
+        F = -self.s * np.einsum("nfe,nea->nfa", g0, J)
+        return u, F
+
+
+def adam_step(p, g, m, v, t, lr, b1=0.9, b2=0.99, eps=1e-15):
+    """One Adam update in place (bias-corrected), as the GPU's optimiser kernel."""
+    m *= b1
+    m += (1 - b1) * g
+    v *= b2
+    v += (1 - b2) * g * g
+    mh = m / (1 - b1 ** t)
+    vh = v / (1 - b2 ** t)
+    p -= lr * mh / (np.sqrt(vh) + eps)
