@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define CCS_ABI_VERSION 1
+#define CCS_ABI_VERSION 2
 
 typedef enum {
   CCS_OK = 0,
@@ -230,6 +230,90 @@ int ccs_get_info(ccs_ctx *ctx, ccs_info *info);
  * FMA-chain kernel over all SMs for about `ms` milliseconds.  The trajectory
  * kernels are bound by the FP32 pipe, so this is their roofline denominator. */
 int ccs_measure_fp32_peak(int device, double ms, double *tflops);
+
+/* ---- Learned field ---------------------------------------------------------
+ * No counterpart in the reference, which evaluates every force of every step
+ * with the linked-cell sums (src/Force.cpp:34-1725); the learned field
+ * replaces those sums where it is trusted.  Per context (target + gas): a
+ * 16-level hash-grid encoding of the site position (2 features per level,
+ * smoothstep blending) feeding an MLP 32 -> 64 -> 64 -> one potential per gas
+ * site type; forces are minus its gradient (a conservative field).  It is
+ * trained on the GPU (ccs_field_train: samples from the context's own exact
+ * evaluator, the project's forward/backward and Adam kernels) and evaluated
+ * in the lane pass by tcgen05 BF16 tensor-core MMAs with FP32 accumulation.
+ * A position is evaluated exactly when it lies within fallback_radius of an
+ * atom, outside the field's domain, or in a voxel whose validation error
+ * exceeds err_threshold.  FP32 precision only. */
+typedef struct {
+  int64_t samples;          /* training samples (default 4,000,000) */
+  int32_t iterations;       /* Adam steps (default 4000) */
+  int32_t batch;            /* samples per step (default 65536) */
+  int32_t log2_table;       /* rows per level = 2^log2_table (default 18, at most 22) */
+  int32_t base_res;         /* coarsest grid resolution over the domain (default 16) */
+  int32_t finest_res;       /* finest grid resolution (default 2048) */
+  int32_t validation;       /* validation samples for the error voxels (default 1,048,576) */
+  double fallback_radius;   /* A: exact evaluation within this distance of any atom (default 3.0) */
+  double voxel;             /* A: edge of the exact-evaluation bitmap's voxels (default 0.5) */
+  double err_voxel;         /* A: edge of the validation-error voxels (default 2.0) */
+  double err_threshold;     /* relative force error |F - F*| / (|F*| + f0) above which a voxel is
+                               evaluated exactly (default 0.05) */
+  double near_fraction;     /* share of samples drawn in the shell around atoms (default 0.5) */
+  double near_shell;        /* A: that shell's thickness beyond fallback_radius (default 6.0) */
+  double lr;                /* Adam learning rate, decayed tenfold over the run (default 1e-2) */
+  double lam_u, u0, f0;     /* loss: lam_u (u-U*)^2/(U*^2+u0^2) + |F-F*|^2/(|F*|^2+f0^2)
+                               (defaults 0.1, 0.05 kcal/mol, 0.05 kcal/mol/A) */
+  uint64_t seed;            /* sampling, initialisation and batch order (default 2104) */
+} ccs_field_params;
+
+typedef struct {
+  double domain_lo[3], domain_side;   /* the field's domain cube, A */
+  int32_t levels, dense_levels, nfields, log2_table;
+  int32_t res[16];                    /* grid resolution per level */
+  int64_t samples;                    /* training samples drawn */
+  double output_scale;                /* s: potentials are s * (network output) */
+  double sample_ms, label_ms, train_ms, validate_ms;
+  double first_loss, final_loss;      /* mean training loss of the first and last steps */
+  double val_force_rel_rms;           /* validation: RMS of |F - F*| / (|F*| + f0) */
+  double val_force_rel_p99;
+  double val_u_abs_rms;               /* RMS |u - U*|, kcal/mol */
+  double exact_fraction;              /* share of the domain's voxels evaluated exactly */
+  int64_t err_voxels;                 /* validation voxels above err_threshold */
+} ccs_field_report;
+
+void ccs_field_params_default(ccs_field_params *p);
+
+/* Sample, label, train and validate the learned field of the context's
+ * current target and parameters (call after ccs_set_target; a later
+ * ccs_set_params or ccs_set_target discards it).  Synchronous.  Does not
+ * switch it on: see ccs_field_enable.  report may be NULL. */
+int ccs_field_train(ccs_ctx *ctx, const ccs_field_params *p, ccs_field_report *report);
+
+/* Runs of this context use the learned field (on = 1) or exact forces only
+ * (on = 0, the default).  CCS_ERR_INVALID if no field is trained. */
+int ccs_field_enable(ccs_ctx *ctx, int on);
+
+/* Inference at npts positions (pos: npts x 3) for gas site `site`: u (npts),
+ * f (npts x 3), and exact[i] = 1 where the trajectory kernels would evaluate
+ * that position exactly (the field's values are still returned).  path 0:
+ * the tensor-core kernel of the lane pass (128 positions per CTA); path 1:
+ * the warp kernel of the warp pass.  exact may be NULL. */
+int ccs_field_eval(ccs_ctx *ctx, size_t npts, int site, const double *pos, int path, double *u, double *f,
+                   int8_t *exact);
+
+/* Test hooks of the training kernels (the checker compares them with its
+ * own restatement).  Parameters in FP32: table [16][2^log2_table][2], mlp =
+ * W1 [64][32], b1 [64], W2 [64][64], b2 [64], W3 [nf][64], b3 [nf].
+ * ccs_field_setup prepares a context's field geometry without training
+ * (domain, grids, exact-evaluation bitmap) with random parameters;
+ * ccs_field_get/set_weights read or replace the parameters (set also
+ * refreshes the inference copies); ccs_field_loss_grad runs the training
+ * forward/backward on n given samples (pos n x 3, labels n x nf x 4: U, Fx,
+ * Fy, Fz) and returns the mean loss and its gradients. */
+int ccs_field_setup(ccs_ctx *ctx, const ccs_field_params *p, ccs_field_report *report);
+int ccs_field_get_weights(ccs_ctx *ctx, float *table, float *mlp, double *output_scale);
+int ccs_field_set_weights(ccs_ctx *ctx, const float *table, const float *mlp, double output_scale);
+int ccs_field_loss_grad(ccs_ctx *ctx, size_t n, const float *pos, const float *labels, double *loss,
+                        float *dtable, float *dmlp);
 
 /* Human-readable strings. */
 const char *ccs_status_string(int status);

@@ -47,18 +47,34 @@ def _run(cmd):
     return r
 
 
+ENGINE_UNITS = ["ccs_engine.cu", "field.cu", "traj_field.cu"]
+ENGINE_HEADERS = ["ccs_device.cuh", "field_device.cuh", "engine_ctx.h"]
+
+
 def build_engine(force=False, verbose=False):
+    """libmassccs_gpu.so from its translation units, compiled in parallel."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIB, exist_ok=True)
+    obj_dir = os.path.join(PKG, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
     out = os.path.join(LIB, "libmassccs_gpu.so")
-    srcs = [os.path.join(CSRC, f) for f in ("ccs_engine.cu", "ccs_device.cuh")] + \
-           [os.path.join(INC, "massccs_gpu.h")]
-    if force or _newer(out, srcs):
-        cmd = [_nvcc()] + ARCH + NVCC_FLAGS + ["-shared", "-o", out, os.path.join(CSRC, "ccs_engine.cu")]
-        if verbose:
-            cmd += ["-Xptxas", "-v"]
-        r = _run(cmd)
-        if verbose:
-            sys.stderr.write(r.stderr)
+    headers = [os.path.join(CSRC, f) for f in ENGINE_HEADERS] + [os.path.join(INC, "massccs_gpu.h")]
+    objs, todo = [], []
+    for u in ENGINE_UNITS:
+        src = os.path.join(CSRC, u)
+        obj = os.path.join(obj_dir, u.replace(".cu", ".o"))
+        objs.append(obj)
+        if force or _newer(obj, [src] + headers):
+            cmd = [_nvcc()] + ARCH + NVCC_FLAGS + ["-c", "-o", obj, src]
+            if verbose:
+                cmd += ["-Xptxas", "-v"]
+            todo.append(cmd)
+    with ThreadPoolExecutor(max_workers=max(1, len(todo))) as ex:
+        for r in ex.map(_run, todo):
+            if verbose:
+                sys.stderr.write(r.stderr)
+    if force or todo or _newer(out, objs):
+        _run([_nvcc()] + ARCH + ["-shared", "-o", out] + objs)
     return out
 
 

@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "field_device.cuh"
+
 namespace ccs {
 
 constexpr int GAS_ATOM = 0;  // He, Ar, "co2": one site
@@ -105,7 +107,8 @@ struct KParams {
   int spec_phase;
   int spec_from;  // failed tries after which a warp-pass trajectory is handed over
   unsigned long long spec_max_parked;  // speculate only when at most this many were parked
-  int *error;                 // 1 = watchdog
+  int *error;                 // 1 = watchdog, 2 = a tensor-core stage timed out
+  FieldK field;               // learned field (field.on == 0: every force exact)
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -116,7 +119,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 // Sets the run's watchdog deadline to now + budget_ns (one thread, enqueued on
 // the run's stream before the trajectory passes).
-__global__ void arm_watchdog(unsigned long long *deadline, unsigned long long budget_ns) {
+static __global__ void arm_watchdog(unsigned long long *deadline, unsigned long long budget_ns) {
   *deadline = global_ns() + budget_ns;
 }
 
@@ -1189,10 +1192,16 @@ __device__ __forceinline__ const KParams *ion_params_ptr(const KParams &kp, cons
   if constexpr (BATCH) return kp.ions + ion; else return kpg;
 }
 
-template <typename T, int G, int GAS, bool HASQ, bool BATCH>
-__global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParams kp, const KParams *__restrict__ kpg) {
+// SURR: the learned field evaluates the probes outside its exact zone (see
+// field_device.cuh): the loop then runs CTA-synchronously, because each step's
+// MLP tile spans the CTA's 128 lanes; probes in the exact zone take the
+// exact path below as before.
+template <typename T, int G, int GAS, bool HASQ, bool BATCH, bool SURR = false>
+__global__ void __launch_bounds__(BLOCK, SURR ? 2 : CCS_LANE_MIN_BLOCKS)
+    traj_kernel(KParams kp, const KParams *__restrict__ kpg) {
   using S = Sites<GAS>;
   constexpr int NS = S::NS;
+  static_assert(!SURR || (sizeof(T) == 4 && !BATCH), "the learned field runs in FP32 single-ion launches");
   constexpr int NSUB = 32 / G;
   constexpr unsigned FULL = 0xffffffffu;
   constexpr int NV = RedShape<GAS>::NV;
@@ -1217,6 +1226,9 @@ __global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParam
   L.ion = 0;
   const unsigned long long deadline = *(volatile const unsigned long long *)kp.deadline;
   bool park_full = false;  // the park buffer filled up: stop asking for slots (it only fills)
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  uint32_t tmem = 0, tc_phase = 0;
+  if constexpr (SURR) tmem = tc_setup(kp.field, tc_smem);
 
   // take trajectories until one hits the ellipsoid (misses are written as free)
   auto grab = [&]() {
@@ -1263,20 +1275,32 @@ __global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParam
         L.mode = M_IDLE;
       }
     }
-    if (__all_sync(FULL, L.mode == M_IDLE)) break;
+    if constexpr (SURR) {
+      if (__syncthreads_and(L.mode == M_IDLE)) break;
+    } else {
+      if (__all_sync(FULL, L.mode == M_IDLE)) break;
+    }
     const KParams &K = ion_params<BATCH>(kp, L.ion);  // this lane's ion
 
     if (L.mode == M_STEP) first_half<T, GAS>(K, L);
 
     // ---- force phase
-    bool near = false;
+    bool near = false, surr = false;
     unsigned actbits = 0;
     T fs[NS][3], Us[NS];
+    T p[NS][3];
     if (L.mode != M_IDLE) {
-      T p[NS][3];
       site_positions<T, GAS>(L, p);
       near = probe_near<T, GAS>(K, p, actbits);
-      if (near) {
+      if constexpr (SURR) {
+        if (near) {
+          surr = true;
+#pragma unroll
+          for (int s = 0; s < NS; s++)
+            if ((actbits >> s) & 1u) surr &= !field_exact(kp.field, (float)p[s][0], (float)p[s][1], (float)p[s][2]);
+        }
+      }
+      if (near && !surr) {
         if constexpr (G == 1) {
           bool act[NS];
 #pragma unroll
@@ -1295,7 +1319,7 @@ __global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParam
     }
     if constexpr (G > 1) {
       __syncwarp();
-      const unsigned bal = __ballot_sync(FULL, near);
+      const unsigned bal = __ballot_sync(FULL, near && !surr);
       const int nn = __popc(bal);
       for (int idx = sub; idx < nn; idx += NSUB) {
         const int t = wbase + nth_set_bit(bal, idx);
@@ -1318,12 +1342,37 @@ __global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParam
         if (g == 0) sm_vis[t] = nv;
       }
       __syncwarp();
-      if (near) {  // the probe's own lane finishes its forces from the raw sums
+      if (near && !surr) {  // the probe's own lane finishes its forces from the raw sums
         bool act[NS];
 #pragma unroll
         for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
         finish_row<T, GAS, HASQ>(K, sm_row[threadIdx.x], act, fs, Us);
         L.nvis += sm_vis[threadIdx.x];
+      }
+    }
+    if constexpr (SURR) {
+      // the learned field for every probe outside the exact zone: one MLP tile
+      // of the CTA's 128 lanes per site
+      if (__syncthreads_or(surr)) {
+        bool ok = true;
+#pragma unroll 1
+        for (int s = 0; s < NS && ok; s++) {
+          const bool use = surr && ((actbits >> s) & 1u);
+          float x[3] = {0.f, 0.f, 0.f};
+          if (use) { x[0] = (float)p[s][0]; x[1] = (float)p[s][1]; x[2] = (float)p[s][2]; }
+          float e[FL_E], J[FL_E][3], u, f3[3];
+          field_encode(kp.field, x, e, J);
+          ok = tc_site(kp.field, tc_smem, tmem, tc_phase, use, e, J, kp.field.site_field[s], u, f3);
+          if (surr) {
+            fs[s][0] = use ? f3[0] : 0.f; fs[s][1] = use ? f3[1] : 0.f; fs[s][2] = use ? f3[2] : 0.f;
+            Us[s] = use ? u : 0.f;
+          }
+        }
+        if (!ok) {  // a tensor-core stage never completed (uniform): stop the kernel
+          if (threadIdx.x == 0) atomicExch(kp.error, 2);
+          if (L.mode != M_IDLE) write_result(K, L, 3, 0.0, blk);
+          break;
+        }
       }
     }
     if (L.mode == M_IDLE) continue;
@@ -1372,6 +1421,7 @@ __global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParam
       }
     }
   }
+  if constexpr (SURR) tc_teardown(tmem);
   __syncthreads();
   if (threadIdx.x < 6 && blk[threadIdx.x]) atomicAdd(&kp.stats[threadIdx.x], blk[threadIdx.x]);
   if (threadIdx.x == 7 && blk[7]) atomicAdd(&kp.stats[6], blk[7]);
@@ -1393,10 +1443,14 @@ __global__ void __launch_bounds__(BLOCK, CCS_LANE_MIN_BLOCKS) traj_kernel(KParam
 // the sequential path.
 constexpr int RBLOCK = 64;  // default threads per trajectory in the warp pass
 
-template <typename T, int GAS, bool HASQ, int NT, bool BATCH>
+// SURR: steps whose sites all lie outside the learned field's exact zone are
+// evaluated by the field, one warp per site (field_site_warp).
+template <typename T, int GAS, bool HASQ, int NT, bool BATCH, bool SURR = false>
 __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_kernel(KParams kp, const KParams *__restrict__ kpg) {
   using S = Sites<GAS>;
   constexpr int NS = S::NS;
+  static_assert(!SURR || (sizeof(T) == 4 && !BATCH), "the learned field runs in FP32 single-ion launches");
+  __shared__ float sm_site[NS][4];
   __shared__ int sm_list[LCAP], sm_wsum[NT / 32];
   __shared__ T sm_red[(NT / 32 + 1) * RedShape<GAS>::P];
   __shared__ unsigned long long blk[8];
@@ -1472,8 +1526,32 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
           bool act[NS];
 #pragma unroll
           for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
-          eval_forces_block<T, NT, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
-                                                tid, sm_list, sm_wsum, sm_red, list_n, list_c, Kg);
+          bool surr = false;  // block-uniform: every thread holds the same state
+          if constexpr (SURR) {
+            surr = true;
+#pragma unroll
+            for (int s = 0; s < NS; s++)
+              if (act[s]) surr &= !field_exact(kp.field, (float)p[s][0], (float)p[s][1], (float)p[s][2]);
+          }
+          if (surr) {
+            for (int s = tid >> 5; s < NS; s += NT / 32) {
+              float u = 0.f, f3[3] = {0.f, 0.f, 0.f};
+              if (act[s]) {
+                const float x[3] = {(float)p[s][0], (float)p[s][1], (float)p[s][2]};
+                field_site_warp(kp.field, x, kp.field.site_field[s], u, f3);
+              }
+              if ((tid & 31) == 0) { sm_site[s][0] = f3[0]; sm_site[s][1] = f3[1]; sm_site[s][2] = f3[2]; sm_site[s][3] = u; }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int s = 0; s < NS; s++) {
+              fs[s][0] = T(sm_site[s][0]); fs[s][1] = T(sm_site[s][1]); fs[s][2] = T(sm_site[s][2]); Us[s] = T(sm_site[s][3]);
+            }
+            __syncthreads();
+          } else {
+            eval_forces_block<T, NT, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
+                                                  tid, sm_list, sm_wsum, sm_red, list_n, list_c, Kg);
+          }
         } else {
 #pragma unroll
           for (int s = 0; s < NS; s++) fs[s][0] = fs[s][1] = fs[s][2] = Us[s] = T(0);
@@ -1624,7 +1702,7 @@ __global__ void __launch_bounds__(BLOCK)
 // Slow probes with small impact parameters run longest (they are the ones
 // captured into orbits and retried); starting them first keeps the longest
 // serial chains off the end of the launch.  Only the order changes, never a result.
-__global__ void order_key_kernel(KParams kp, float *key, uint32_t *idx) {
+static __global__ void order_key_kernel(KParams kp, float *key, uint32_t *idx) {
   const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= kp.ntraj) return;
   const double v = vel_sample(kp, kp.rnd[kp.rnd_stride + j]);
@@ -1635,7 +1713,7 @@ __global__ void order_key_kernel(KParams kp, float *key, uint32_t *idx) {
 }
 
 // Initial conditions (ccs_eval_setup): one thread per trajectory.
-__global__ void setup_kernel(KParams kp, int8_t *hit, double *pos, double *vel) {
+static __global__ void setup_kernel(KParams kp, int8_t *hit, double *pos, double *vel) {
   const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= kp.ntraj) return;
   Init I;

@@ -21,98 +21,15 @@
 
 #include <cub/device/device_radix_sort.cuh>
 
-#include "../../include/massccs_gpu.h"
-#include "ccs_device.cuh"
+#include "engine_ctx.h"
 
 using namespace ccs;
 
-struct ccs_ctx {
-  int device = 0;
-  int sm_count = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev[10] = {};  // [0..4] ccs_run, [5..7] passes, [8..9] autotuner
-  ccs_params p{};
-  bool have_params = false, have_target = false;
-  std::string err;
-  // engine grid
-  int nx = 0, ny = 0, nz = 0, natoms = 0, max_cell = 0;
-  double h = 0, origin[3] = {0, 0, 0}, bb_lo[3] = {0, 0, 0}, bb_hi[3] = {0, 0, 0}, reach = 0;
-  int charged = 0, allpairs = 0, coul_on = 0, dip_on = 0;
-  float4 *d_xyzq32 = nullptr;
-  float2 *d_ab32 = nullptr, *d_abc32 = nullptr;
-  double4 *d_xyzq64 = nullptr;
-  double2 *d_ab64 = nullptr, *d_abc64 = nullptr;
-  int *d_cell_start = nullptr;
-  // speed table
-  double *d_vtab_v = nullptr, *d_vtab_s = nullptr;
-  int vtab_n = 0;
-  // per-run scratch
-  unsigned long long *d_work = nullptr;  // [0] work counter, [1..7] stats, [8] clock, [9] parked, [10] resumed
-  int *d_error = nullptr;
-  double *d_rnd = nullptr;
-  size_t rnd_cap = 0;
-  int8_t *d_status = nullptr;
-  double *d_omc = nullptr;
-  uint32_t *d_steps = nullptr, *d_visits = nullptr;
-  size_t out_cap = 0;
-  // longest-first processing order
-  float *d_key = nullptr, *d_key2 = nullptr;
-  uint32_t *d_idx = nullptr, *d_idx2 = nullptr;
-  void *d_sort_tmp = nullptr;
-  size_t order_cap = 0, sort_tmp_bytes = 0;
-  // parked long trajectories (lane pass -> warp pass)
-  void *d_park = nullptr;
-  size_t park_bytes = 0;
-  // speculative retries: records and try outcomes
-  SpecRec *d_spec_rec = nullptr;
-  SpecOut *d_spec_out = nullptr;
-  size_t spec_cap = 0;
-  // device copy of the launch parameters (read by the non-inlined set-up code)
-  KParams *d_kparams = nullptr;
-  KParams h_kparams{};
-  // batched runs led by this context: the ions' parameters and first trajectories
-  KParams *d_bkp = nullptr;
-  unsigned long long *d_bstart = nullptr;
-  size_t bkp_cap = 0;
-  int batch_G = 0;                        // tuned lanes for the last batch shape
-  size_t batch_nions = 0, batch_total = 0;
-  // launch choice
-  int tuned_G = 0, tuned_block = 0;
-  ccs_stats last{};
-  // where the last run keeps its counters and error flag (the context's own
-  // buffers, or the static scratch of ccs_run_device_noalloc)
-  unsigned long long *run_work = nullptr;
-  int *run_error = nullptr;
-};
-
 namespace {
-
-int fail(ccs_ctx *c, int code, const char *fmt, ...) {
-  if (c) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, sizeof buf, fmt, ap);
-    va_end(ap);
-    c->err = buf;
-  }
-  return code;
-}
-
-#define CK(call)                                                                       \
-  do {                                                                                 \
-    cudaError_t e_ = (call);                                                           \
-    if (e_ != cudaSuccess)                                                             \
-      return fail(c, CCS_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),    \
-                  __FILE__, __LINE__);                                                 \
-  } while (0)
-
-template <typename P> void dfree(P *&p) {
-  if (p) cudaFree((void *)p);
-  p = nullptr;
-}
+using namespace ccs_internal;
 
 void free_target(ccs_ctx *c) {
+  field_free(c);  // the learned field belongs to this target and these parameters
   dfree(c->d_xyzq32); dfree(c->d_ab32); dfree(c->d_abc32);
   dfree(c->d_xyzq64); dfree(c->d_ab64); dfree(c->d_abc64);
   dfree(c->d_cell_start);
@@ -121,8 +38,6 @@ void free_target(ccs_ctx *c) {
   c->batch_G = 0;
 }
 
-bool is_molecule(int gas) { return gas == CCS_GAS_N2 || gas == CCS_GAS_CO2; }
-int gas_kind(int gas) { return gas == CCS_GAS_N2 ? GAS_N2 : gas == CCS_GAS_CO2 ? GAS_CO2 : GAS_ATOM; }
 
 // GasBuffer::gas_properties (GasBuffer.cpp:58-192): site charges, masses, z offsets.
 void gas_table(int gas, double q[3], double m[3], double z[3], double &mass) {
@@ -167,7 +82,6 @@ void vel_table(double m_amu, double T, std::vector<double> &V, std::vector<doubl
   }
 }
 
-using KernelFn = void (*)(KParams, const KParams *);
 template <typename T, int GAS, bool HASQ> KernelFn resume_ptr(int nt) {
   return nt == 32 ? resume_kernel<T, GAS, HASQ, 32, false>
                   : nt == 64 ? resume_kernel<T, GAS, HASQ, 64, false> : resume_kernel<T, GAS, HASQ, 128, false>;
@@ -239,7 +153,9 @@ ForceFn pick_force(const ccs_ctx *c, int G) {
                                          : pick_force_t<float>(gas, hasq, g_index(G));
 }
 
-KParams base_params(const ccs_ctx *c) {
+}  // namespace
+
+KParams ccs_internal::base_params(const ccs_ctx *c) {
   const ccs_params &p = c->p;
   KParams k;
   std::memset(&k, 0, sizeof k);
@@ -310,6 +226,8 @@ KParams base_params(const ccs_ctx *c) {
   k.error = c->d_error;
   return k;
 }
+
+namespace {
 
 // Speculative-retry buffers for up to cap records (the park capacity) and
 // the counters d_work[11] (records) and d_work[12] (next speculative try).
@@ -396,9 +314,14 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   k.steps = d_steps;
   k.visits = d_visits;
   int rc = CCS_OK;
-  KernelFn fn = pick_traj(c, G);
+  field_kparams(c, k);  // the learned field, when on
+  const bool surr = k.field.on != 0;
+  const bool hasq = c->coul_on || c->dip_on;
+  KernelFn fn = surr ? pick_traj_field(gas_kind(c->p.gas), hasq, G) : pick_traj(c, G);
+  const int dyn = surr ? TC_SMEM_BYTES : 0;  // the MLP tiles of the lane pass
+  if (surr) CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, dyn));
   if (per_sm < 1) per_sm = 1;
   size_t grid = (size_t)per_sm * c->sm_count;
   const size_t max_useful = (n + block - 1) / block;  // one trajectory per lane
@@ -457,11 +380,12 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   c->h_kparams = k;
   CK(cudaMemcpyAsync(c->d_kparams, &c->h_kparams, sizeof(KParams), cudaMemcpyHostToDevice, s));
   CK(cudaEventRecord(c->ev[5], s));
-  fn<<<(unsigned)grid, block, 0, s>>>(k, c->d_kparams);
+  fn<<<(unsigned)grid, block, dyn, s>>>(k, c->d_kparams);
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev[6], s));
   // warp pass over the parked trajectories (exits at once when none were parked)
-  rc = launch_warp_pass<false>(c, pick_resume(c), resume_threads(c), k, s);
+  KernelFn rfn = surr ? pick_resume_field(gas_kind(c->p.gas), hasq, resume_threads(c)) : pick_resume(c);
+  rc = launch_warp_pass<false>(c, rfn, resume_threads(c), k, s);
   if (rc) return rc;
   CK(cudaEventRecord(c->ev[7], s));
   c->last.grid_size = (int32_t)grid;
@@ -491,6 +415,7 @@ int read_stats(ccs_ctx *c, ccs_stats *st, size_t n) {
   c->last.steps = h[4]; c->last.visits = h[5]; c->last.parked = h[6];
   c->last.speculated = work == c->d_work ? (int32_t)std::min<unsigned long long>(h[10], c->spec_cap) : 0;
   if (st) *st = c->last;
+  if (herr == 2) return fail(c, CCS_ERR_CUDA, "a tensor-core stage of the learned field did not complete");
   if (herr) return fail(c, CCS_ERR_TIMEOUT, "device watchdog expired after %.0f s",
                         c->p.watchdog_s > 0 ? c->p.watchdog_s : 600.0);
   return CCS_OK;
@@ -1175,6 +1100,18 @@ const char *ccs_status_string(int s) {
 const char *ccs_last_error(ccs_ctx *c) { return c ? c->err.c_str() : "no context"; }
 
 }  // extern "C"
+
+int ccs_internal::eval_site_forces_device(ccs_ctx *c, size_t npts, int site, const double *d_pos, double *d_f,
+                                          double *d_U, cudaStream_t s) {
+  if (npts == 0) return CCS_OK;
+  KParams k = base_params(c);
+  ForceFn fn = pick_force(c, 32);
+  const int block = 128;
+  const size_t grid = std::min<size_t>((npts * 32 + block - 1) / block, (size_t)c->sm_count * 16);
+  fn<<<(unsigned)grid, block, 0, s>>>(k, site, npts, d_pos, d_f, d_U, nullptr);
+  CK(cudaGetLastError());
+  return CCS_OK;
+}
 
 // ===========================================================================
 // ccs_run_device_noalloc: the trajectory passes with no device allocation.

@@ -70,11 +70,44 @@ class CcsInfo(ctypes.Structure):
         return d
 
 
+class CcsFieldParams(ctypes.Structure):
+    _fields_ = [
+        ("samples", ctypes.c_int64), ("iterations", ctypes.c_int32), ("batch", ctypes.c_int32),
+        ("log2_table", ctypes.c_int32), ("base_res", ctypes.c_int32), ("finest_res", ctypes.c_int32),
+        ("validation", ctypes.c_int32),
+        ("fallback_radius", ctypes.c_double), ("voxel", ctypes.c_double), ("err_voxel", ctypes.c_double),
+        ("err_threshold", ctypes.c_double), ("near_fraction", ctypes.c_double), ("near_shell", ctypes.c_double),
+        ("lr", ctypes.c_double), ("lam_u", ctypes.c_double), ("u0", ctypes.c_double), ("f0", ctypes.c_double),
+        ("seed", ctypes.c_uint64),
+    ]
+
+
+class CcsFieldReport(ctypes.Structure):
+    _fields_ = [
+        ("domain_lo", ctypes.c_double * 3), ("domain_side", ctypes.c_double),
+        ("levels", ctypes.c_int32), ("dense_levels", ctypes.c_int32), ("nfields", ctypes.c_int32),
+        ("log2_table", ctypes.c_int32), ("res", ctypes.c_int32 * 16),
+        ("samples", ctypes.c_int64), ("output_scale", ctypes.c_double),
+        ("sample_ms", ctypes.c_double), ("label_ms", ctypes.c_double), ("train_ms", ctypes.c_double),
+        ("validate_ms", ctypes.c_double), ("first_loss", ctypes.c_double), ("final_loss", ctypes.c_double),
+        ("val_force_rel_rms", ctypes.c_double), ("val_force_rel_p99", ctypes.c_double),
+        ("val_u_abs_rms", ctypes.c_double), ("exact_fraction", ctypes.c_double), ("err_voxels", ctypes.c_int64),
+    ]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["domain_lo"] = list(self.domain_lo)
+        d["res"] = list(self.res)
+        return d
+
+
 # Every symbol include/massccs_gpu.h declares.
 EXPORTS = ["ccs_version", "ccs_create", "ccs_destroy", "ccs_params_default", "ccs_set_target",
            "ccs_set_params", "ccs_run", "ccs_run_device", "ccs_sync_stats", "ccs_eval_site_forces",
            "ccs_eval_setup", "ccs_get_info", "ccs_status_string", "ccs_last_error",
-           "ccs_measure_fp32_peak", "ccs_run_device_noalloc", "ccs_run_batch"]
+           "ccs_measure_fp32_peak", "ccs_run_device_noalloc", "ccs_run_batch",
+           "ccs_field_params_default", "ccs_field_train", "ccs_field_enable", "ccs_field_eval",
+           "ccs_field_setup", "ccs_field_get_weights", "ccs_field_set_weights", "ccs_field_loss_grad"]
 
 _LIB = None
 
@@ -111,9 +144,29 @@ def load_library(path=LIB_PATH):
     L.ccs_run_device_noalloc.argtypes = [vp, sz, vp, sz, vp, vp, vp, vp, vp, ctypes.POINTER(CcsStats)]
     L.ccs_run_batch.argtypes = [ctypes.POINTER(vp), sz, ctypes.POINTER(sz), ctypes.POINTER(vp), vp, vp, vp, vp,
                                 ctypes.POINTER(CcsStats)]
+    L.ccs_field_params_default.argtypes = [ctypes.POINTER(CcsFieldParams)]
+    L.ccs_field_params_default.restype = None
+    L.ccs_field_train.argtypes = [vp, ctypes.POINTER(CcsFieldParams), ctypes.POINTER(CcsFieldReport)]
+    L.ccs_field_setup.argtypes = [vp, ctypes.POINTER(CcsFieldParams), ctypes.POINTER(CcsFieldReport)]
+    L.ccs_field_enable.argtypes = [vp, i32]
+    L.ccs_field_eval.argtypes = [vp, sz, i32, vp, i32, vp, vp, vp]
+    L.ccs_field_get_weights.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_double)]
+    L.ccs_field_set_weights.argtypes = [vp, vp, vp, ctypes.c_double]
+    L.ccs_field_loss_grad.argtypes = [vp, sz, vp, vp, ctypes.POINTER(ctypes.c_double), vp, vp]
     if path == LIB_PATH:
         _LIB = L
     return L
+
+
+def field_params(**kw):
+    """ccs_field_params with the library's defaults, then the given fields."""
+    p = CcsFieldParams()
+    load_library().ccs_field_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
 
 
 def _p(a):
@@ -225,6 +278,67 @@ class Engine:
         st = CcsStats()
         self._check(self._L.ccs_sync_stats(self._h, ctypes.byref(st)), "ccs_sync_stats")
         return st.as_dict()
+
+    # ---- learned field
+    def field_train(self, **kw):
+        """ccs_field_train with the default parameters overridden by kw; returns the report."""
+        p = field_params(**kw)
+        r = CcsFieldReport()
+        self._check(self._L.ccs_field_train(self._h, ctypes.byref(p), ctypes.byref(r)), "ccs_field_train")
+        self.field_nf = r.nfields
+        self.field_log2 = r.log2_table
+        return r.as_dict()
+
+    def field_setup(self, **kw):
+        p = field_params(**kw)
+        r = CcsFieldReport()
+        self._check(self._L.ccs_field_setup(self._h, ctypes.byref(p), ctypes.byref(r)), "ccs_field_setup")
+        self.field_nf = r.nfields
+        self.field_log2 = r.log2_table
+        return r.as_dict()
+
+    def field_enable(self, on=True):
+        self._check(self._L.ccs_field_enable(self._h, 1 if on else 0), "ccs_field_enable")
+
+    def field_eval(self, site, pos, path=0):
+        """(u, f, exact) of the learned field at pos (n x 3); path 0 tensor cores, 1 warp."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        n = pos.shape[0]
+        u = np.empty(n)
+        f = np.empty((n, 3))
+        ex = np.empty(n, dtype=np.int8)
+        self._check(self._L.ccs_field_eval(self._h, n, site, _p(pos), path, _p(u), _p(f), _p(ex)), "ccs_field_eval")
+        return u, f, ex
+
+    def _field_sizes(self):
+        nt = 16 * (1 << self.field_log2) * 2
+        nm = 64 * 32 + 64 + 64 * 64 + 64 + self.field_nf * 64 + self.field_nf
+        return nt, nm
+
+    def field_get_weights(self):
+        nt, nm = self._field_sizes()
+        t = np.empty(nt, dtype=np.float32)
+        m = np.empty(nm, dtype=np.float32)
+        s = ctypes.c_double()
+        self._check(self._L.ccs_field_get_weights(self._h, _p(t), _p(m), ctypes.byref(s)), "ccs_field_get_weights")
+        return t.reshape(16, -1, 2), m, s.value
+
+    def field_set_weights(self, table, mlp, scale):
+        t = np.ascontiguousarray(table, dtype=np.float32)
+        m = np.ascontiguousarray(mlp, dtype=np.float32)
+        self._check(self._L.ccs_field_set_weights(self._h, _p(t), _p(m), float(scale)), "ccs_field_set_weights")
+
+    def field_loss_grad(self, pos, labels):
+        """Mean loss and its gradients (table [16][T][2], mlp vector) on the given samples."""
+        pos = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
+        lab = np.ascontiguousarray(labels, dtype=np.float32)
+        nt, nm = self._field_sizes()
+        dt = np.empty(nt, dtype=np.float32)
+        dm = np.empty(nm, dtype=np.float32)
+        loss = ctypes.c_double()
+        self._check(self._L.ccs_field_loss_grad(self._h, pos.shape[0], _p(pos), _p(lab), ctypes.byref(loss),
+                                                _p(dt), _p(dm)), "ccs_field_loss_grad")
+        return loss.value, dt.reshape(16, -1, 2), dm
 
     def eval_site_forces(self, site, pos, want_visits=True):
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)

@@ -40,7 +40,7 @@ def test_cli_is_built():
 
 def test_abi_version_and_strings(lib):
     v = ctypes.c_int32(0)
-    assert lib.ccs_version(ctypes.byref(v)) == 0 and v.value == 1
+    assert lib.ccs_version(ctypes.byref(v)) == 0 and v.value == 2
     assert lib.ccs_status_string(0) == b"ok"
     assert lib.ccs_status_string(-4) == b"device watchdog expired"
     assert lib.ccs_last_error(None) == b"no context"
@@ -74,6 +74,7 @@ def test_ctypes_layouts_match_the_headers(tmp_path):
     from massccs_b200 import engine, host
     cc = shutil.which("gcc") or "/usr/bin/gcc"
     mirrors = {"ccs_params": engine.CcsParams, "ccs_stats": engine.CcsStats, "ccs_info": engine.CcsInfo,
+               "ccs_field_params": engine.CcsFieldParams, "ccs_field_report": engine.CcsFieldReport,
                "mh_info": host.MhInfo}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "massccs_gpu.h"', '#include "massccs_host.h"',
              "int main(void) {"]
@@ -92,3 +93,12 @@ def test_ctypes_layouts_match_the_headers(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_field_params_defaults(lib):
+    """The learned field's defaults are the stated configuration: 16 levels of
+    2^18 rows, resolutions 16..2048, 4e6 samples, exact within 3 A of an atom."""
+    from massccs_b200 import engine
+    p = engine.field_params()
+    assert (p.samples, p.log2_table, p.base_res, p.finest_res) == (4000000, 18, 16, 2048)
+    assert (p.fallback_radius, p.voxel, p.err_threshold) == (3.0, 0.5, 0.05)
