@@ -61,6 +61,12 @@ CONFIGS = {
     "batch_he": dict(gen="batch", gas="He", ft=4,
                      desc="batched ions: globules of 500-50000 atoms (log-uniform), net charge 0-30 e, He, "
                           "force type 4; one ccs_run_batch call per step"),
+    "field_n2": dict(gen="field_globule", gas="N2", ft=6, ntraj=100000, nprobe=100000, niter=10,
+                     desc="learned field: 20,000-atom globule (+12 e), N2 3-site, force type 6; "
+                          "plain FP32 and the learned field on the same trajectories"),
+    "field_co2": dict(gen="field_globule", gas="CO2", ft=6, ntraj=100000, nprobe=100000, niter=10,
+                      desc="learned field: 20,000-atom globule (+12 e), CO2 3-site, force type 6; "
+                           "plain FP32 and the learned field on the same trajectories"),
 }
 
 
@@ -72,6 +78,8 @@ def make_workload(name, d):
     from massccs_b200 import synth
     c = CONFIGS[name]
     gen = getattr(synth, c["gen"])
+    if c["gen"] == "field_globule":
+        return gen(d, gas=c["gas"], nprobe=c["nprobe"], niter=c["niter"])
     return gen(d, nprobe=c["nprobe"], niter=c["niter"])
 
 
@@ -357,6 +365,115 @@ def run_batch_bench(args, rank, world, local):
     shutil.rmtree(d, ignore_errors=True)
 
 
+def run_field_bench(args, rank, world, local):
+    """field_n2 / field_co2: the learned-field configuration.  The field is
+    trained once (its set-up cost is reported, not timed as a step); each
+    timed step runs the step's trajectories with plain FP32 forces and with
+    the learned field, from the same device-resident random rows; accuracy:
+    both against the FP64 plain path on the same initial conditions."""
+    import numpy as np
+    import torch
+    from massccs_b200 import host as H
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    cfg = CONFIGS[args.config]
+    d = tempfile.mkdtemp(prefix=f"bench_field_{rank}_")
+    json_path = make_workload(args.config, d)
+    S = H.System(json_path)
+    n = args.ntraj if args.ntraj > 0 else cfg["ntraj"]
+    seed = S.info["seed"] + rank
+    rnd_host = S.predraw(n, seed=seed)
+    eng = S.engine(device=local)
+    t0 = time.perf_counter()
+    rep = eng.field_train(**({"samples": args.field_samples} if args.field_samples else {}),
+                          **({"iterations": args.field_iters} if args.field_iters else {}))
+    train_s = time.perf_counter() - t0
+    log(f"[rank {rank}] field trained in {train_s:.1f} s: " + json.dumps(
+        {k: rep[k] for k in ("sample_ms", "label_ms", "train_ms", "validate_ms", "first_loss", "final_loss",
+                             "val_force_rel_rms", "val_force_rel_p99", "exact_fraction", "err_voxels")}))
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    d_rnd = torch.from_numpy(rnd_host).to(dev)
+    d_status = torch.empty(n, dtype=torch.int8, device=dev)
+    d_omc = torch.empty(n, dtype=torch.float64, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def timed(on):
+        eng.field_enable(on)
+        for _ in range(args.warmup):
+            eng.run_device(n, d_rnd.data_ptr(), n, d_status.data_ptr(), d_omc.data_ptr(), 0, 0, stream.cuda_stream)
+        torch.cuda.synchronize()
+        ms, st = [], None
+        for _ in range(args.steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            eng.run_device(n, d_rnd.data_ptr(), n, d_status.data_ptr(), d_omc.data_ptr(), 0, 0, stream.cuda_stream)
+            b.record(stream)
+            st = eng.sync_stats()
+            ms.append(a.elapsed_time(b))
+        return sum(ms) / len(ms), st, d_status.cpu().numpy(), d_omc.cpu().numpy()
+
+    with ClockSampler(local) as clocks:
+        plain_ms, plain_st, p_status, p_omc = timed(False)
+        field_ms, field_st, f_status, f_omc = timed(True)
+    # e2e with the field on: host rows in, results out, through ccs_run
+    eng.field_enable(True)
+    t1 = time.perf_counter()
+    for _ in range(args.steps):
+        o = eng.run(rnd_host, want_steps=False, want_visits=False)
+        H.reduce(1, n, o["status"], o["one_minus_cos"], S.info["bmax"])
+    e2e_s = (time.perf_counter() - t1) / args.steps
+    line = None
+    if rank == 0:
+        bmax = S.info["bmax"]
+        m = min(n, args.fp64_check if args.fp64_check > 0 else 20000)
+        e64 = S.engine(device=local, precision=1)
+        r64 = e64.run(np.ascontiguousarray(rnd_host[:, :m]), want_steps=False, want_visits=False)
+        e64.close()
+
+        def paired(status, omc):
+            a = np.pi * np.where(r64["status"] == 1, r64["one_minus_cos"], 0.0) * bmax ** 2
+            b = np.pi * np.where(status[:m] == 1, omc[:m], 0.0) * bmax ** 2
+            ok = (r64["status"] <= 1) & (status[:m] <= 1)
+            dd = (b - a)[ok]
+            ref = float(a[ok].mean())
+            return {"ccs_fp64_A2": ref, "ccs_A2": float(b[ok].mean()), "rel_diff": float(dd.mean() / ref),
+                    "rel_se": float(dd.std(ddof=1) / np.sqrt(len(dd)) / ref),
+                    "status_agreement": float((r64["status"] == status[:m]).mean())}
+        acc = {"trajectories": int(m), "vs": "FP64 plain engine mode, same initial conditions (paired)",
+               "plain_fp32": paired(p_status, p_omc), "field": paired(f_status, f_omc)}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu, _ = cpu_baseline(json_path, args.config)
+        value = world * n / (field_ms * 1e-3)
+        line = {
+            "metric": METRIC, "value": value, "unit": "trajectories/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": field_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 forces/integration, bf16 MLP with f32 accumulation", "data": "synthetic",
+            "config": {"workload": args.config, "description": cfg["desc"], "trajectories_per_gpu": n,
+                       "l2": "256 MiB buffer written between timed steps (outside the step events)"},
+            "plain_fp32": {"value": world * n / (plain_ms * 1e-3), "ms_per_step": plain_ms,
+                           "lane_ms": plain_st["lane_ms"], "warp_ms": plain_st["warp_ms"],
+                           "visits_per_traj": plain_st["visits"] / n},
+            "field": {"value": value, "ms_per_step": field_ms, "lane_ms": field_st["lane_ms"],
+                      "warp_ms": field_st["warp_ms"], "exact_visits_per_traj": field_st["visits"] / n,
+                      "gain_over_plain": plain_ms / field_ms},
+            "training": {"wall_s": train_s, **{k: rep[k] for k in (
+                "samples", "sample_ms", "label_ms", "train_ms", "validate_ms", "first_loss", "final_loss",
+                "val_force_rel_rms", "val_force_rel_p99", "val_u_abs_rms", "exact_fraction", "err_voxels")}},
+            "e2e": {"value": world * n / e2e_s, "unit": "trajectories/s",
+                    "h2d_bytes_per_step": 9 * 8 * n, "d2h_bytes_per_step": 9 * n,
+                    "includes": "ccs_run with the learned field (H2D, both passes, D2H) and the reduction; "
+                                "training excluded (set-up, in `training`)"},
+            "accuracy": acc, "cpu_baseline": cpu, "gpu_launches": 6 * args.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    shutil.rmtree(d, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -371,6 +488,8 @@ def main():
                     help="trajectories rerun in FP64 mode to report the FP32 CCS error (-1: all, 0: skip)")
     ap.add_argument("--ions", type=int, default=256, help="batch_he: number of ions")
     ap.add_argument("--traj-per-ion", type=int, default=20000, help="batch_he: trajectories per ion")
+    ap.add_argument("--field-samples", type=int, default=0, help="field_*: training samples (0: default)")
+    ap.add_argument("--field-iters", type=int, default=0, help="field_*: training steps (0: default)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -381,6 +500,9 @@ def main():
         return
     if args.config == "batch_he":
         run_batch_bench(args, rank, world, local)
+        return
+    if args.config.startswith("field_"):
+        run_field_bench(args, rank, world, local)
         return
     dist = None
     if world > 1:

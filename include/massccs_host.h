@@ -71,6 +71,20 @@ int mh_reduce(size_t niter, size_t nprobe, const int8_t *status, const double *o
 int mh_run(mh_system *sys, int device, const ccs_params *overrides, int print, double *ccs,
            double *err, double *seconds);
 
+/* The same run as one job split over several GPUs (no counterpart in the
+ * reference, whose OpenMP loop shares one host's cores): one pre-draw,
+ * contiguous slices of the trajectory numbers per GPU (one context and one
+ * host thread each), the reduction in the reference's fixed order over all of
+ * them.  Every trajectory keeps its random numbers, so the result equals the
+ * one-GPU run's whenever the lanes per force evaluation agree: with
+ * lanes_per_traj = 0 they are tuned once, on the first GPU, and used by all.
+ * A GPU number may repeat (several contexts on one GPU). */
+int mh_run_devices(mh_system *sys, size_t ndevices, const int *devices, const ccs_params *overrides, int print,
+                   double *ccs, double *err, double *seconds);
+
+/* The GPUs the input.json's "devices" key names (count 0: the key is absent). */
+int mh_get_devices(const mh_system *sys, int *devices, size_t cap, size_t *count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,12 +1,14 @@
 // capi.cpp -- the C-ABI of include/massccs_host.h over the host set-up, and
 // mh_run: the reference's whole run (System.cpp:19-326) with the trajectory
 // loop replaced by ccs_run.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <iostream>
 #include <memory>
+#include <thread>
 #include <vector>
 
 #include "massccs_host.h"
@@ -120,22 +122,19 @@ int mh_reduce(size_t niter, size_t nprobe, const int8_t *status, const double *o
   return CCS_OK;
 }
 
-int mh_run(mh_system *sys, int device, const ccs_params *overrides, int print, double *ccs_out, double *err_out,
-           double *seconds) {
-  if (!sys) return CCS_ERR_INVALID;
-  const auto &S = *sys->S;
-  const size_t niter = S.in.nIter, nprobe = S.in.nProbe, n = niter * nprobe;
-  if (n == 0) return CCS_ERR_INVALID;
-  ccs_params p;
-  if (overrides) p = *overrides;
-  else mh_fill_params(sys, &p);
+}  // extern "C"
+
+namespace {
+using CtxPtr = std::unique_ptr<ccs_ctx, void (*)(ccs_ctx *)>;
+
+int make_context(const massccs::SystemSetup &S, int device, const ccs_params &p, CtxPtr &out, int print) {
   ccs_ctx *ctx = nullptr;
   int rc = ccs_create(&ctx, device);
   if (rc) {
-    if (print) std::cerr << "ccs_create: " << ccs_status_string(rc) << std::endl;
+    if (print) std::cerr << "ccs_create (GPU " << device << "): " << ccs_status_string(rc) << std::endl;
     return rc;
   }
-  std::unique_ptr<ccs_ctx, void (*)(ccs_ctx *)> guard(ctx, ccs_destroy);
+  out.reset(ctx);
   if ((rc = ccs_set_params(ctx, &p)) ||
       (rc = ccs_set_target(ctx, (size_t)S.target.natoms, S.target.x.data(), S.target.y.data(), S.target.z.data(),
                            S.target.q.data(), S.target.eps.data(), S.target.sig.data(),
@@ -144,6 +143,30 @@ int mh_run(mh_system *sys, int device, const ccs_params *overrides, int print, d
     if (print) std::cerr << "massccs: " << ccs_last_error(ctx) << std::endl;
     return rc;
   }
+  return CCS_OK;
+}
+
+// The whole run over one or several GPUs: one pre-draw, contiguous slices of
+// the trajectory numbers per GPU (every trajectory keeps its random numbers,
+// so the split changes no initial condition), one fixed-order reduction.
+// With several GPUs the lanes per force evaluation are tuned once (GPU 0, on
+// the run's first trajectories) and used by every GPU.
+int run_impl(mh_system *sys, const std::vector<int> &devices, const ccs_params *overrides, int print,
+             double *ccs_out, double *err_out, double *seconds) {
+  const auto &S = *sys->S;
+  const size_t niter = S.in.nIter, nprobe = S.in.nProbe, n = niter * nprobe;
+  if (n == 0 || devices.empty()) return CCS_ERR_INVALID;
+  const size_t nd = devices.size();
+  ccs_params p;
+  if (overrides) p = *overrides;
+  else mh_fill_params(sys, &p);
+  std::vector<CtxPtr> ctxs;
+  for (size_t r = 0; r < nd; r++) {
+    ctxs.emplace_back(nullptr, ccs_destroy);
+    int rc = make_context(S, devices[r], p, ctxs.back(), print);
+    if (rc) return rc;
+  }
+  ccs_ctx *ctx = ctxs[0].get();
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<double> rnd(9 * n);
   massccs::predraw(S, S.in.seed, n, rnd.data());
@@ -157,7 +180,55 @@ int mh_run(mh_system *sys, int device, const ccs_params *overrides, int print, d
   std::vector<int8_t> status(n);
   std::vector<double> omc(n);
   ccs_stats st;
-  if ((rc = ccs_run(ctx, n, rows, status.data(), omc.data(), nullptr, nullptr, &st))) {
+  std::memset(&st, 0, sizeof st);
+  int rc = CCS_OK;
+  if (nd == 1) {
+    rc = ccs_run(ctx, n, rows, status.data(), omc.data(), nullptr, nullptr, &st);
+  } else {
+    if (p.lanes_per_traj == 0) {  // tune once, on GPU 0, then fix the choice everywhere
+      const size_t m = std::min<size_t>(n, 148 * 256);
+      std::vector<int8_t> s0(m);
+      std::vector<double> o0(m);
+      ccs_info info;
+      if ((rc = ccs_run(ctx, m, rows, s0.data(), o0.data(), nullptr, nullptr, nullptr)) ||
+          (rc = ccs_get_info(ctx, &info))) {
+        if (print) std::cerr << "massccs: " << ccs_last_error(ctx) << std::endl;
+        return rc;
+      }
+      p.lanes_per_traj = info.reserved;  // the tuned lanes per force evaluation
+      for (size_t r = 0; r < nd; r++)
+        if ((rc = make_context(S, devices[r], p, ctxs[r], print))) return rc;
+      ctx = ctxs[0].get();
+    }
+    std::vector<ccs_stats> sts(nd);
+    std::vector<int> rcs(nd, CCS_OK);
+    std::vector<std::thread> th;
+    for (size_t r = 0; r < nd; r++) {
+      th.emplace_back([&, r]() {
+        const size_t lo = n * r / nd, hi = n * (r + 1) / nd;
+        const double *rr[9];
+        for (int k = 0; k < 9; k++) rr[k] = rows[k] + lo;
+        rcs[r] = hi > lo ? ccs_run(ctxs[r].get(), hi - lo, rr, status.data() + lo, omc.data() + lo, nullptr, nullptr,
+                                   &sts[r])
+                         : CCS_OK;
+      });
+    }
+    for (auto &t : th) t.join();
+    for (size_t r = 0; r < nd; r++) {
+      if (rcs[r]) {
+        if (print) std::cerr << "massccs (GPU " << devices[r] << "): " << ccs_last_error(ctxs[r].get()) << std::endl;
+        return rcs[r];
+      }
+      const ccs_stats &a = sts[r];
+      st.ntraj += a.ntraj; st.nfree += a.nfree; st.nscatter += a.nscatter; st.nlost += a.nlost;
+      st.ncapped += a.ncapped; st.steps += a.steps; st.visits += a.visits; st.parked += a.parked;
+      st.kernel_ms = std::max(st.kernel_ms, a.kernel_ms);
+      st.lane_ms = std::max(st.lane_ms, a.lane_ms);
+      st.warp_ms = std::max(st.warp_ms, a.warp_ms);
+      st.lanes_per_traj = a.lanes_per_traj;
+    }
+  }
+  if (rc) {
     if (print) std::cerr << "massccs: " << ccs_last_error(ctx) << std::endl;
     return rc;
   }
@@ -177,10 +248,11 @@ int mh_run(mh_system *sys, int device, const ccs_params *overrides, int print, d
     std::cout << "average value of CCS = " << R.ccs << " Ang^2" << std::endl;
     std::cout << "error value of CCS = " << R.err << " Ang^2" << std::endl;
     std::cout << "*********************************************************" << std::endl;
-    std::cout << "B200 engine: " << (p.precision == CCS_PREC_FP64 ? "FP64" : "FP32") << ", "
-              << st.lanes_per_traj << " lanes per force evaluation, " << st.kernel_ms << " ms on the device ("
-              << st.lane_ms << " lane pass, " << st.warp_ms << " warp pass, " << st.parked
-              << " long trajectories), " << (double)n / (st.kernel_ms * 1e-3) << " trajectories/s" << std::endl;
+    std::cout << "B200 engine: " << (p.precision == CCS_PREC_FP64 ? "FP64" : "FP32") << ", " << nd
+              << (nd == 1 ? " GPU, " : " GPUs, ") << st.lanes_per_traj << " lanes per force evaluation, "
+              << st.kernel_ms << " ms on the device (" << st.lane_ms << " lane pass, " << st.warp_ms
+              << " warp pass, " << st.parked << " long trajectories), " << (double)n / (st.kernel_ms * 1e-3)
+              << " trajectories/s" << std::endl;
     if (st.ncapped)
       std::cout << "warning: " << st.ncapped << " trajectories reached the step cap and were counted as lost"
                 << std::endl;
@@ -226,6 +298,29 @@ int mh_run(mh_system *sys, int device, const ccs_params *overrides, int print, d
   if (ccs_out) *ccs_out = R.ccs;
   if (err_out) *err_out = R.err;
   if (seconds) *seconds = secs;
+  return CCS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int mh_run(mh_system *sys, int device, const ccs_params *overrides, int print, double *ccs_out, double *err_out,
+           double *seconds) {
+  if (!sys) return CCS_ERR_INVALID;
+  return run_impl(sys, std::vector<int>{device}, overrides, print, ccs_out, err_out, seconds);
+}
+
+int mh_run_devices(mh_system *sys, size_t ndevices, const int *devices, const ccs_params *overrides, int print,
+                   double *ccs_out, double *err_out, double *seconds) {
+  if (!sys || ndevices == 0 || !devices) return CCS_ERR_INVALID;
+  return run_impl(sys, std::vector<int>(devices, devices + ndevices), overrides, print, ccs_out, err_out, seconds);
+}
+
+int mh_get_devices(const mh_system *sys, int *devices, size_t cap, size_t *count) {
+  if (!sys || !count) return CCS_ERR_INVALID;
+  const auto &d = sys->S->in.devices;
+  *count = d.size();
+  for (size_t k = 0; k < d.size() && k < cap && devices; k++) devices[k] = d[k];
   return CCS_OK;
 }
 

@@ -138,6 +138,27 @@ Input::Input(const std::string &path) {
       throw std::invalid_argument("precision must be fp32 or fp64");
   }
   if (has("fp64_check")) fp64_check = unsigned_number(d["fp64_check"], "fp64_check");
+  if (has("devices")) {  // one job split over several GPUs: a count, or a comma-separated list of GPU numbers
+    const std::string &t = d["devices"].text;
+    devices.clear();
+    if (t.find(',') == std::string::npos) {
+      const unsigned nd = unsigned_number(d["devices"], "devices");
+      for (unsigned k = 0; k < nd; k++) devices.push_back((int)k);
+    } else {
+      size_t s = 0;
+      while (s <= t.size()) {
+        const size_t e = std::min(t.find(',', s), t.size());
+        const std::string item = t.substr(s, e - s);
+        size_t used = 0;
+        int v = -1;
+        try { v = std::stoi(item, &used); } catch (const std::exception &) { used = 0; }
+        if (used == 0 || used != item.size() || v < 0) throw std::invalid_argument("Error input.json: devices format error");
+        devices.push_back(v);
+        s = e + 1;
+      }
+    }
+    if (devices.empty()) throw std::invalid_argument("Error input.json: devices must name at least one GPU");
+  }
 }
 
 void Input::print() const {

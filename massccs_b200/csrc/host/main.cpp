@@ -1,5 +1,6 @@
 // main.cpp -- the drop-in CLI: `massccs input.json` (cces-cepid/massccs
 // src/main.cpp:20-34) with the trajectory loop on the B200.
+#include <algorithm>
 #include <chrono>
 #include <iostream>
 
@@ -18,7 +19,11 @@ int main(int argc, char *argv[]) {
     std::cerr << "massccs: " << err << std::endl;
     return 1;
   }
-  rc = mh_run(sys, 0, nullptr, 1, nullptr, nullptr, nullptr);
+  int devs[64];
+  size_t nd = 0;
+  mh_get_devices(sys, devs, 64, &nd);  // "devices" in input.json: one job over several GPUs
+  rc = nd > 1 ? mh_run_devices(sys, std::min<size_t>(nd, 64), devs, nullptr, 1, nullptr, nullptr, nullptr)
+              : mh_run(sys, nd == 1 ? devs[0] : 0, nullptr, 1, nullptr, nullptr, nullptr);
   mh_close(sys);
   if (rc) {
     std::cerr << "massccs: " << ccs_status_string(rc) << std::endl;

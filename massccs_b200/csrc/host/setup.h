@@ -24,6 +24,7 @@ struct Input {
   bool ref_quirks = false;   // extension key "ref_quirks": reproduce the CO2 reference-velocity bug
   std::string precision = "fp32";  // extension key "precision": "fp32" or "fp64"
   unsigned fp64_check = 2000;      // extension key "fp64_check": FP32 runs rerun this many trajectories in FP64
+  std::vector<int> devices;        // extension key "devices": a count N (GPUs 0..N-1) or a list "0,2,3"
 
   explicit Input(const std::string &path);
   void print() const;  // Input::printReadInput (Input.cpp:313-345)

@@ -16,7 +16,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "lib", "libmassccs_host.so")
 
 EXPORTS = ["mh_open", "mh_close", "mh_get_info", "mh_get_target", "mh_fill_params", "mh_predraw",
-           "mh_reduce", "mh_run"]
+           "mh_reduce", "mh_run", "mh_run_devices", "mh_get_devices"]
 
 
 class MhInfo(ctypes.Structure):
@@ -65,6 +65,8 @@ def load_library():
         L.mh_predraw.argtypes = [vp, ctypes.c_uint32, sz, vp]
         L.mh_reduce.argtypes = [sz, sz, vp, vp, ctypes.c_double, vp, vp, vp, vp, vp, vp]
         L.mh_run.argtypes = [vp, ctypes.c_int, ctypes.POINTER(E.CcsParams), ctypes.c_int, vp, vp, vp]
+        L.mh_run_devices.argtypes = [vp, ctypes.c_size_t, vp, ctypes.POINTER(E.CcsParams), ctypes.c_int, vp, vp, vp]
+        L.mh_get_devices.argtypes = [vp, vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         _LIB = L
     return _LIB
 
@@ -138,6 +140,24 @@ class System:
         if rc != 0:
             raise E.CcsError(f"mh_run failed: {rc}")
         return ccs.value, err.value, secs.value
+
+    def run_devices(self, devices, print_report=False, **overrides):
+        """The whole run as one job split over the given GPUs -> (ccs, err, seconds)."""
+        p = self.params(**overrides)
+        devs = (ctypes.c_int * len(devices))(*devices)
+        ccs, err, secs = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        rc = self._L.mh_run_devices(self._h, len(devices), devs, ctypes.byref(p), int(print_report),
+                                    ctypes.byref(ccs), ctypes.byref(err), ctypes.byref(secs))
+        if rc != 0:
+            raise E.CcsError(f"mh_run_devices failed: {rc}")
+        return ccs.value, err.value, secs.value
+
+    def devices(self):
+        """The GPUs named by input.json's "devices" key ([] when absent)."""
+        buf = (ctypes.c_int * 64)()
+        n = ctypes.c_size_t()
+        self._L.mh_get_devices(self._h, buf, 64, ctypes.byref(n))
+        return list(buf[:min(n.value, 64)])
 
 
 def reduce(niter, nprobe, status, omc, bmax):

@@ -173,3 +173,13 @@ def test_equipotential_ellipsoid_matches_reference_binary(host, target, gas, ft)
     for k, r in zip("abc", ref):
         assert abs(S.info[k] - r) <= 6e-6 * r, (k, S.info[k], r)
     assert S.info["bmax"] == max(S.info["a"], S.info["b"], S.info["c"])
+
+
+def test_devices_key(host):
+    """input.json's "devices" extension key: a count (GPUs 0..N-1) or a list."""
+    d = workdir()
+    assert host.System(write_input(d, input_dict("c60.xyz"), name="a.json")).devices() == []
+    assert host.System(write_input(d, dict(input_dict("c60.xyz"), devices=3), name="b.json")).devices() == [0, 1, 2]
+    assert host.System(write_input(d, dict(input_dict("c60.xyz"), devices="0,2,2"), name="c.json")).devices() == [0, 2, 2]
+    with pytest.raises(Exception, match="devices"):
+        host.System(write_input(d, dict(input_dict("c60.xyz"), devices="0,x"), name="e.json"))
