@@ -43,10 +43,14 @@ REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 REF_SAMPLE = 30000  # fewest trajectories per timed reference sample
 
 
-def ref_sample_size(rs, total):
+def ref_sample_size(rs, total, cap=None):
     """Trajectories per timed reference sample: at least REF_SAMPLE and about
-    10 s of CPU work, at most the workload's own count."""
-    return int(min(total, max(REF_SAMPLE, rs["probe_rate"] * 10.0)) // 10 * 10)
+    10 s of CPU work, at most the workload's own count (and, for the large
+    assembly, the subset size its configuration states)."""
+    n = min(total, max(REF_SAMPLE, rs["probe_rate"] * 10.0))
+    if cap:
+        n = min(n, cap)
+    return int(n // 10 * 10)
 
 # flops per target-atom visit of one probe site (fixed constants of the work
 # model): LJ + induced dipole 45, LJ + Coulomb 25, Coulomb + induced dipole 40,
@@ -61,6 +65,12 @@ CONFIGS = {
     "batch_he": dict(gen="batch", gas="He", ft=4,
                      desc="batched ions: globules of 500-50000 atoms (log-uniform), net charge 0-30 e, He, "
                           "force type 4; one ccs_run_batch call per step"),
+    "shell_he": dict(gen="shell", gas="He", ft=4, ntraj=1000000, nprobe=100000, niter=10, ref_max=10000,
+                     desc="large assembly: 5e5-atom spherical shell (r 100-130 A, +40 e), He, force type 4, "
+                          "1e6 trajectories; the reference timed on a 1e4-trajectory subset"),
+    "shell_n2": dict(gen="shell", gas="N2", ft=6, ntraj=100000, nprobe=10000, niter=10, ref_max=2000,
+                     desc="large assembly: 5e5-atom spherical shell (r 100-130 A, +40 e), N2 3-site, force type 6, "
+                          "1e5 trajectories per step; the reference timed on a 2e3-trajectory subset"),
     "field_n2": dict(gen="field_globule", gas="N2", ft=6, ntraj=100000, nprobe=100000, niter=10,
                      desc="learned field: 20,000-atom globule (+12 e), N2 3-site, force type 6; "
                           "plain FP32 and the learned field on the same trajectories"),
@@ -78,7 +88,7 @@ def make_workload(name, d):
     from massccs_b200 import synth
     c = CONFIGS[name]
     gen = getattr(synth, c["gen"])
-    if c["gen"] == "field_globule":
+    if c["gen"] in ("field_globule", "shell"):
         return gen(d, gas=c["gas"], nprobe=c["nprobe"], niter=c["niter"])
     return gen(d, nprobe=c["nprobe"], niter=c["niter"])
 
@@ -186,7 +196,7 @@ def ref_sample_run(binary, json_path, nprobe, niter, threads):
     return nprobe * niter, float(m.group(1)), float(c.group(1)) if c else None
 
 
-def ref_setup(json_path):
+def ref_setup(json_path, probe_n=2000):
     """Binary, thread count and sample shape of the timed reference runs: the
     faster of all physical cores and all logical CPUs on a probe sample of
     2000 trajectories (the reference's results do not depend on it)."""
@@ -196,7 +206,7 @@ def ref_setup(json_path):
         return None
     best = None
     for threads in sorted({cpu["physical_cores"], cpu["logical_cpus"]}):
-        n0, t0, _ = ref_sample_run(binary, json_path, 200, 10, threads)
+        n0, t0, _ = ref_sample_run(binary, json_path, max(1, probe_n // 10), 10, threads)
         rate = n0 / max(t0, 1e-3)
         if best is None or rate > best[1]:
             best = (threads, rate)
@@ -217,10 +227,11 @@ def cpu_baseline(json_path, config):
     algorithmic work."""
     out = {"value": None, "unit": "trajectories/s", "cores": None, "kind": "reference", "sample": None}
     visits = None
-    rs = ref_setup(json_path)
+    cap = CONFIGS[config].get("ref_max")
+    rs = ref_setup(json_path, probe_n=min(2000, cap // 5) if cap else 2000)
     if rs:
         niter = 10
-        nprobe = ref_sample_size(rs, CONFIGS[config].get("ntraj", REF_SAMPLE)) // niter
+        nprobe = ref_sample_size(rs, CONFIGS[config].get("ntraj", REF_SAMPLE), CONFIGS[config].get("ref_max")) // niter
         n, t, _ = ref_sample_run(rs["binary"], json_path, nprobe, niter, rs["threads"])
         out.update(value=n / t, cores=rs["threads"], isa=rs["isa"], cpu=rs["cpu"],
                    sample=ref_describe(rs, n, nprobe, niter, f"; CCS time {t:.2f} s"))
@@ -270,9 +281,10 @@ def run_reference_arm(args, rank, world):
         return
     d = tempfile.mkdtemp(prefix="bench_ref_")
     json_path = make_workload(args.config, d)
-    rs = ref_setup(json_path)
+    cap = cfg.get("ref_max")
+    rs = ref_setup(json_path, probe_n=min(2000, cap // 5) if cap else 2000)
     niter = 10
-    nprobe = ref_sample_size(rs, cfg.get("ntraj", REF_SAMPLE)) // niter  # >= 3e4 trajectories per timed step
+    nprobe = ref_sample_size(rs, cfg.get("ntraj", REF_SAMPLE), cfg.get("ref_max")) // niter  # >= 3e4 per step
     for _ in range(args.warmup):  # warm-up steps at a tenth of the size
         ref_sample_run(rs["binary"], json_path, nprobe // 10, niter, rs["threads"])
     times, n = [], 0
@@ -524,8 +536,11 @@ def main():
     json_path = make_workload(args.config, d)
     S = H.System(json_path)
     n = args.ntraj if args.ntraj > 0 else cfg["ntraj"]
-    seed = S.info["seed"] + rank  # each rank its own trajectories
-    rnd_host = S.predraw(n, seed=seed)
+    # one job of world * n trajectories from one pre-draw; rank r runs the
+    # contiguous slice [r n, (r + 1) n) (weak scaling: n per GPU is fixed)
+    seed = S.info["seed"]
+    job = world * n
+    rnd_host = np.ascontiguousarray(S.predraw(job, seed=seed)[:, rank * n:(rank + 1) * n])
     eng = S.engine(device=local)
     stream = torch.cuda.Stream(dev)  # a real stream handle (0 would mean the engine's own stream)
     torch.cuda.set_stream(stream)
@@ -575,23 +590,34 @@ def main():
 
     # e2e through the public API: pre-draw on the host into pinned memory,
     # ccs_run (H2D, both passes, D2H), the reduction; every step
-    pin = torch.empty((9, n), dtype=torch.float64).pin_memory()
+    pin = torch.empty((9, job), dtype=torch.float64).pin_memory()
     pin_np = pin.numpy()
     st_pin = torch.empty(n, dtype=torch.int8).pin_memory().numpy()
     om_pin = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
-    rows = (__import__("ctypes").c_void_p * 9)(*[pin_np[k].ctypes.data for k in range(9)])
     import ctypes
+    # this rank's slice of the job's rows
+    rows = (ctypes.c_void_p * 9)(*[pin_np[k].ctypes.data + 8 * rank * n for k in range(9)])
+    if dist:  # per-trajectory results of every rank, gathered for the fixed-order reduction
+        g_st = torch.empty(job, dtype=torch.int8, device=dev)
+        g_om = torch.empty(job, dtype=torch.float64, device=dev)
     L = E.load_library()
     HL = H.load_library()
 
     def step_e2e():
-        HL.mh_predraw(S._h, seed, n, pin_np.ctypes.data_as(ctypes.c_void_p))
+        HL.mh_predraw(S._h, seed, job, pin_np.ctypes.data_as(ctypes.c_void_p))
         stt = E.CcsStats()
         rc = L.ccs_run(eng._h, n, rows, st_pin.ctypes.data_as(ctypes.c_void_p),
                        om_pin.ctypes.data_as(ctypes.c_void_p), None, None, ctypes.byref(stt))
         if rc:
             raise E.CcsError(L.ccs_last_error(eng._h).decode())
-        H.reduce(S.info["niter"], S.info["nprobe"], st_pin, om_pin, S.info["bmax"])
+        if dist:
+            dist.all_gather_into_tensor(g_st, torch.from_numpy(st_pin).to(dev))
+            dist.all_gather_into_tensor(g_om, torch.from_numpy(om_pin).to(dev))
+            if rank == 0:
+                H.reduce(S.info["niter"] * world, S.info["nprobe"], g_st.cpu().numpy(), g_om.cpu().numpy(),
+                         S.info["bmax"])
+        else:
+            H.reduce(S.info["niter"], S.info["nprobe"], st_pin, om_pin, S.info["bmax"])
 
     step_e2e()
     barrier()
@@ -634,10 +660,12 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.config, "description": cfg["desc"], "trajectories_per_gpu": n,
                        "l2": "256 MiB buffer written between timed steps (outside the step events)",
-                       "parallelism": f"{world} ranks, independent trajectory shards"},
+                       "parallelism": f"one job of {world} x {n} trajectories (one pre-draw), rank r runs "
+                                      f"trajectories [r n, (r+1) n); results gathered to rank 0 for the "
+                                      f"fixed-order reduction"},
             "e2e": {"value": e2e_value, "unit": "trajectories/s",
                     "h2d_bytes_per_step": (9 if cfg["gas"] in ("N2", "CO2") else 5) * 8 * n,  # rows ccs_run copies
-                    "d2h_bytes_per_step": 9 * n,
+                    "d2h_bytes_per_step": 9 * n * (world if world > 1 else 1),
                     "includes": "host mt19937 pre-draw, H2D, lane+warp passes, D2H, reduction"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,

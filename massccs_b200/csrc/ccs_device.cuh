@@ -187,13 +187,28 @@ template <int GAS> __device__ __forceinline__ constexpr bool site_coul(int s) {
   return GAS != GAS_ATOM;  // atomic probes are neutral
 }
 
-// Accumulators of one fused force evaluation.
+// Accumulators of one fused force evaluation.  In FP32 the site energies
+// are summed with Kahan compensation (Uc holds each sum's running rounding
+// error): the energy test compares totals of ~1e3 terms to 0.5-1 %, so their
+// rounding must stay far below that.
 template <typename T, int NS> struct Acc {
-  T f[NS][3], U[NS];
+  T f[NS][3], U[NS], Uc[NS];
   T E[3], G[6];  // field and symmetric gradient (xx yy zz xy xz yz) at the dipole site
+  __device__ __forceinline__ void addU(int s, T v) {
+    if constexpr (sizeof(T) == 4) {
+      const T y = v - Uc[s];
+      const T t = U[s] + y;
+      Uc[s] = (t - U[s]) - y;
+      U[s] = t;
+    } else {
+      U[s] += v;
+    }
+  }
+  // the compensated sum of site s
+  __device__ __forceinline__ T Usum(int s) const { return sizeof(T) == 4 ? U[s] - Uc[s] : U[s]; }
   __device__ __forceinline__ void zero() {
 #pragma unroll
-    for (int s = 0; s < NS; s++) { f[s][0] = f[s][1] = f[s][2] = U[s] = T(0); }
+    for (int s = 0; s < NS; s++) { f[s][0] = f[s][1] = f[s][2] = U[s] = Uc[s] = T(0); }
 #pragma unroll
     for (int k = 0; k < 3; k++) E[k] = T(0);
 #pragma unroll
@@ -222,6 +237,7 @@ __device__ __forceinline__ void visit_atom(const KParams &kp, const T (&p)[GasSh
 #pragma unroll
   for (int s = 0; s < NS; s++) {
     if (!act[s]) continue;
+    T us = T(0);  // this pair's energy at site s (one compensated addition per site)
     const T dx = p[s][0] - a.x, dy = p[s][1] - a.y, dz = p[s][2] - a.z;
     const T r2 = dx * dx + dy * dy + dz * dz;
     const int lj = site_lj<GAS>(s);
@@ -234,7 +250,7 @@ __device__ __forceinline__ void visit_atom(const KParams &kp, const T (&p)[GasSh
       const T ir6 = ir2 * ir2 * ir2;
       const T u = ir6 * (A * ir6 - B) - (A * T(kp.rc12inv) - B * T(kp.rc6inv));
       const T fl = in_lj ? ir6 * (T(12) * A * ir6 - T(6) * B) * ir2 : T(0);
-      acc.U[s] += in_lj ? u : T(0);
+      us += in_lj ? u : T(0);
       acc.f[s][0] += fl * dx; acc.f[s][1] += fl * dy; acc.f[s][2] += fl * dz;
     }
     if constexpr (HASQ) {
@@ -245,7 +261,7 @@ __device__ __forceinline__ void visit_atom(const KParams &kp, const T (&p)[GasSh
         const T kq = T(KCOUL * kp.q_site[s]) * a.q;
         const T u = kq * (ir - T(kp.c1) + T(kp.c2) * r2);
         const T fc = in_c ? kq * (ir3 - T(kp.rc3inv)) : T(0);
-        acc.U[s] += in_c ? u : T(0);
+        us += in_c ? u : T(0);
         acc.f[s][0] += fc * dx; acc.f[s][1] += fc * dy; acc.f[s][2] += fc * dz;
       }
       if (s == GasShape<GAS>::DIP && kp.dip_on) {
@@ -262,6 +278,7 @@ __device__ __forceinline__ void visit_atom(const KParams &kp, const T (&p)[GasSh
         acc.G[5] += ty * dz;
       }
     }
+    acc.addU(s, us);
   }
 }
 
@@ -319,7 +336,7 @@ __device__ __forceinline__ int column_range(const KParams &kp, T cx, T cy, T Rr,
 // Raw sums of one force evaluation, in row order: per site f (3) and U, then
 // the field (3) and its gradient (xx yy zz xy xz yz) at the dipole site.
 template <typename T, int NS> __device__ __forceinline__ T acc_value(const Acc<T, NS> &acc, int k) {
-  return k < 4 * NS ? (k % 4 == 3 ? acc.U[k / 4] : acc.f[k / 4][k % 4])
+  return k < 4 * NS ? (k % 4 == 3 ? acc.Usum(k / 4) : acc.f[k / 4][k % 4])
                     : (k < 4 * NS + 3 ? acc.E[k - 4 * NS] : acc.G[k - 4 * NS - 3]);
 }
 
@@ -683,7 +700,7 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
   T v[P];
 #pragma unroll
   for (int s = 0; s < NS; s++) {
-    v[4 * s] = acc.f[s][0]; v[4 * s + 1] = acc.f[s][1]; v[4 * s + 2] = acc.f[s][2]; v[4 * s + 3] = acc.U[s];
+    v[4 * s] = acc.f[s][0]; v[4 * s + 1] = acc.f[s][1]; v[4 * s + 2] = acc.f[s][2]; v[4 * s + 3] = acc.Usum(s);
   }
 #pragma unroll
   for (int k = 0; k < 3; k++) v[4 * NS + k] = acc.E[k];
@@ -1471,9 +1488,10 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
   }
   unsigned long long *next = spec ? kp.spec_next : kp.park_next;
   // speculation pays when the warp pass is bound by its longest chains of
-  // tries, not when parked trajectories outnumber the CTAs (then the extra
-  // tries only add work)
-  const bool may_spec = kp.spec_rec && !spec && np <= kp.spec_max_parked;
+  // tries, not while parked trajectories wait for a CTA (then the extra
+  // tries only add work): a failed try is handed over when few trajectories
+  // were parked at all, or once every parked trajectory has been taken
+  const bool may_spec = kp.spec_rec && !spec;
   for (;;) {
     if (tid == 0) sm_idx = *(volatile int *)kp.error ? np : atomicAdd(next, 1ull);
     __syncthreads();
@@ -1594,7 +1612,8 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
       }
       if (may_spec && L.tries >= kp.spec_from) {  // hand the remaining tries to the speculative phase
         if (tid == 0) {
-          const unsigned long long slot = atomicAdd(kp.spec_count, 1ull);
+          const bool drained = np <= kp.spec_max_parked || *(volatile unsigned long long *)kp.park_next >= np;
+          const unsigned long long slot = drained ? atomicAdd(kp.spec_count, 1ull) : ~0ull;
           sm_idx = slot;
           if (slot < kp.spec_cap) {
             SpecRec R;
