@@ -315,6 +315,22 @@ int ccs_field_set_weights(ccs_ctx *ctx, const float *table, const float *mlp, do
 int ccs_field_loss_grad(ccs_ctx *ctx, size_t n, const float *pos, const float *labels, double *loss,
                         float *dtable, float *dmlp);
 
+/* The equipotential ellipsoid's boundary points on the GPU
+ * (src/Equipotential.cpp:86-200 with the all-atom potentials of :203-557):
+ * the z-extent march from (0, 0, |max_z| + 20) in 0.5 A steps, then
+ * max(25, ceil(zmax)) + 1 z-levels of 20 rays towards the z-axis in 0.1 A
+ * steps; each step's potential is an FP64 sum over all atoms (one CTA per
+ * ray, fixed-order reduction).  Threshold ek in kcal/mol; alpha in kcal/mol
+ * units; eps/sig as for ccs_set_target (eps_c/sig_c for CO2).  Writes every
+ * ray's crossing point (0, 0, 0: none) in (level, rotation) order into pts
+ * (cap rows of 3) and their count into npts (CCS_ERR_INVALID with npts set
+ * when cap is too small); zmax receives the widened z extent (x 1.3).  The
+ * least-squares fit is the caller's (the host library does it). */
+int ccs_equipotential_points(int device, size_t natoms, const double *x, const double *y, const double *z,
+                             const double *q, const double *eps, const double *sig, const double *eps_c,
+                             const double *sig_c, int gas, int polar, double alpha, double ek, double max_x,
+                             double max_y, double max_z, size_t cap, double *pts, size_t *npts, double *zmax);
+
 /* Human-readable strings. */
 const char *ccs_status_string(int status);
 const char *ccs_last_error(ccs_ctx *ctx);

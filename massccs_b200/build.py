@@ -47,7 +47,7 @@ def _run(cmd):
     return r
 
 
-ENGINE_UNITS = ["ccs_engine.cu", "field.cu", "traj_field.cu"]
+ENGINE_UNITS = ["ccs_engine.cu", "field.cu", "traj_field.cu", "setup_gpu.cu"]
 ENGINE_HEADERS = ["ccs_device.cuh", "field_device.cuh", "engine_ctx.h"]
 
 

@@ -24,6 +24,7 @@
 #include <iostream>
 #include <vector>
 
+#include "massccs_gpu.h"
 #include "setup.h"
 
 namespace massccs {
@@ -115,7 +116,8 @@ double norm3(const double p[3]) { return std::sqrt(p[0] * p[0] + p[1] * p[1] + p
 }  // namespace
 
 void equipotential_ellipsoid(const MoleculeTarget &t, int gas, int polarizability_flag, double temperature,
-                             double mu, double alpha, int nthreads, bool print, double &a, double &b, double &c) {
+                             double mu, double alpha, int nthreads, bool print, double &a, double &b, double &c,
+                             int gpu_device) {
   const Probe U{t, gas, polarizability_flag != 0, alpha};
   // the energy threshold (Equipotential.cpp:31-37)
   const double v_mb = 2.0 * std::sqrt((2.0 * kB * temperature) / (M_PI * mu * kAmuKg));
@@ -123,57 +125,75 @@ void equipotential_ellipsoid(const MoleculeTarget &t, int gas, int polarizabilit
   const double v_min = v_mb - 2.0 * std::sqrt(v2_mb - v_mb * v_mb);
   const double ek = 0.01 * (0.5 * mu * kAmuKg * std::pow(v_min, 2.0) * kJeV * kEvKcal);
 
-  // extent along z (:86-120)
-  double pos[3] = {0.0, 0.0, std::fabs(t.maxZ) + 20.0}, prev[3];
-  double slope = (U(pos) + ek < 0.0) ? -1.0 : 1.0;
-  double zMax = 0.0;
-  for (;;) {
-    std::copy(pos, pos + 3, prev);
-    pos[2] -= 0.5 * slope;
-    if ((U(pos) + ek) * slope < 0.0) {
-      zMax = std::max(pos[2], prev[2]);
-      break;
-    }
-  }
-
-  // rays towards the z-axis on every z-level (:122-200)
-  const int nrot = 20;
-  const double velMag = 0.1;
-  zMax *= 1.3;
-  const double posMag = std::fabs(std::max(std::fabs(t.maxX), std::fabs(t.maxY))) + std::fabs(zMax - std::fabs(t.maxZ));
-  const int levels = (int)std::ceil((double)std::max(25, (int)std::ceil(zMax)));
-  const double zInc = 2 * zMax / levels;
-  // every ray is independent: they run in parallel, each in sequence, and
-  // the points keep the reference's (level, rotation) order
-  const int nrays = (levels + 1) * nrot;
-  std::vector<std::array<double, 3>> hits((size_t)nrays, std::array<double, 3>{0.0, 0.0, 0.0});
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
-  for (int ray = 0; ray < nrays; ray++) {
-    const int i = ray / nrot, n = ray % nrot;
-    const double zPos = -zMax + i * zInc;
-    const double theta = n * 2.0 * M_PI / (double)nrot;
-    const double startX = posMag * std::cos(theta), startY = posMag * std::sin(theta);
-    double p[3] = {startX, startY, zPos}, pp[3] = {0.0, 0.0, 0.0};
-    double vel[3] = {-velMag * std::cos(theta), -velMag * std::sin(theta), 0.0};
-    const double s = (U(p) + ek < 0.0) ? -1.0 : 1.0;  // inside the boundary: search outwards
-    for (double &v : vel) v *= s;
+  std::vector<std::array<double, 3>> pts;
+  if (gpu_device >= 0) {
+    // the marches on the GPU (ccs_equipotential_points): the same rays and
+    // rules, each step's all-atom potential summed there
+    const size_t cap = 64 * 20 + (size_t)(1.3 * (std::fabs(t.maxZ) + 20.0) + 64) * 20 * 4;
+    std::vector<double> hits(3 * cap);
+    size_t nh = 0;
+    double zm = 0.0;
+    const int rc = ccs_equipotential_points(gpu_device, (size_t)t.natoms, t.x.data(), t.y.data(), t.z.data(),
+                                            t.q.data(), t.eps.data(), t.sig.data(),
+                                            gas == 3 ? t.eps_c.data() : nullptr, gas == 3 ? t.sig_c.data() : nullptr,
+                                            gas, polarizability_flag, alpha, ek, t.maxX, t.maxY, t.maxZ, cap,
+                                            hits.data(), &nh, &zm);
+    if (rc) throw std::runtime_error(std::string("equipotential on the GPU: ") + ccs_status_string(rc));
+    for (size_t k = 0; k < nh; k++)
+      if (!(hits[3 * k] == 0 && hits[3 * k + 1] == 0 && hits[3 * k + 2] == 0))
+        pts.push_back({hits[3 * k], hits[3 * k + 1], hits[3 * k + 2]});
+  } else {
+    // extent along z (:86-120)
+    double pos[3] = {0.0, 0.0, std::fabs(t.maxZ) + 20.0}, prev[3];
+    double slope = (U(pos) + ek < 0.0) ? -1.0 : 1.0;
+    double zMax = 0.0;
     for (;;) {
-      if ((U(p) + ek) * s < 0.0) {
-        const double *far = norm3(pp) > norm3(p) ? pp : p;  // the crossing step's farther point
-        hits[(size_t)ray] = {far[0], far[1], far[2]};
+      std::copy(pos, pos + 3, prev);
+      pos[2] -= 0.5 * slope;
+      if ((U(pos) + ek) * slope < 0.0) {
+        zMax = std::max(pos[2], prev[2]);
         break;
       }
-      // crossed to the other side of the molecule without meeting the boundary
-      if ((startX == 0 && startY / p[1] <= 0) || (startY == 0 && startX / p[0] <= 0) ||
-          (startX / p[0] <= 0 && startY / p[1] <= 0))
-        break;
-      std::copy(p, p + 3, pp);
-      for (int k = 0; k < 3; k++) p[k] += vel[k];
     }
+
+    // rays towards the z-axis on every z-level (:122-200)
+    const int nrot = 20;
+    const double velMag = 0.1;
+    zMax *= 1.3;
+    const double posMag = std::fabs(std::max(std::fabs(t.maxX), std::fabs(t.maxY))) + std::fabs(zMax - std::fabs(t.maxZ));
+    const int levels = (int)std::ceil((double)std::max(25, (int)std::ceil(zMax)));
+    const double zInc = 2 * zMax / levels;
+    // every ray is independent: they run in parallel, each in sequence, and
+    // the points keep the reference's (level, rotation) order
+    const int nrays = (levels + 1) * nrot;
+    std::vector<std::array<double, 3>> hits((size_t)nrays, std::array<double, 3>{0.0, 0.0, 0.0});
+  #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int ray = 0; ray < nrays; ray++) {
+      const int i = ray / nrot, n = ray % nrot;
+      const double zPos = -zMax + i * zInc;
+      const double theta = n * 2.0 * M_PI / (double)nrot;
+      const double startX = posMag * std::cos(theta), startY = posMag * std::sin(theta);
+      double p[3] = {startX, startY, zPos}, pp[3] = {0.0, 0.0, 0.0};
+      double vel[3] = {-velMag * std::cos(theta), -velMag * std::sin(theta), 0.0};
+      const double s = (U(p) + ek < 0.0) ? -1.0 : 1.0;  // inside the boundary: search outwards
+      for (double &v : vel) v *= s;
+      for (;;) {
+        if ((U(p) + ek) * s < 0.0) {
+          const double *far = norm3(pp) > norm3(p) ? pp : p;  // the crossing step's farther point
+          hits[(size_t)ray] = {far[0], far[1], far[2]};
+          break;
+        }
+        // crossed to the other side of the molecule without meeting the boundary
+        if ((startX == 0 && startY / p[1] <= 0) || (startY == 0 && startX / p[0] <= 0) ||
+            (startX / p[0] <= 0 && startY / p[1] <= 0))
+          break;
+        std::copy(p, p + 3, pp);
+        for (int k = 0; k < 3; k++) p[k] += vel[k];
+      }
+    }
+    for (const auto &h : hits)
+      if (!(h[0] == 0 && h[1] == 0 && h[2] == 0)) pts.push_back(h);
   }
-  std::vector<std::array<double, 3>> pts;
-  for (const auto &h : hits)
-    if (!(h[0] == 0 && h[1] == 0 && h[2] == 0)) pts.push_back(h);
 
   // least-squares ellipsoid through the points (:560-640)
   double m4[3] = {0, 0, 0}, m22[3] = {0, 0, 0}, m2[3] = {0, 0, 0};  // x4 y4 z4; x2y2 x2z2 y2z2; x2 y2 z2

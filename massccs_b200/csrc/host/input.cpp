@@ -138,6 +138,11 @@ Input::Input(const std::string &path) {
       throw std::invalid_argument("precision must be fp32 or fp64");
   }
   if (has("fp64_check")) fp64_check = unsigned_number(d["fp64_check"], "fp64_check");
+  if (has("setup_device")) {
+    setup_device = d["setup_device"].text;
+    if (setup_device != "cpu" && setup_device != "gpu" && setup_device != "auto")
+      throw std::invalid_argument("setup_device must be cpu, gpu or auto");
+  }
   if (has("devices")) {  // one job split over several GPUs: a count, or a comma-separated list of GPU numbers
     const std::string &t = d["devices"].text;
     devices.clear();

@@ -25,6 +25,8 @@ struct Input {
   std::string precision = "fp32";  // extension key "precision": "fp32" or "fp64"
   unsigned fp64_check = 2000;      // extension key "fp64_check": FP32 runs rerun this many trajectories in FP64
   std::vector<int> devices;        // extension key "devices": a count N (GPUs 0..N-1) or a list "0,2,3"
+  std::string setup_device = "auto";  // extension key "setup_device": where the equipotential rays run:
+                                      // "cpu", "gpu", or "auto" (the GPU from 20,000 atoms on)
 
   explicit Input(const std::string &path);
   void print() const;  // Input::printReadInput (Input.cpp:313-345)
@@ -93,7 +95,8 @@ struct SystemSetup {
 // the equipotential ellipsoid (Equipotential.cpp:19-715): a, b, c of the
 // surface where the probe's potential is 1 % of a slow particle's kinetic energy
 void equipotential_ellipsoid(const MoleculeTarget &t, int gas, int polarizability_flag, double temperature,
-                             double mu, double alpha, int nthreads, bool print, double &a, double &b, double &c);
+                             double mu, double alpha, int nthreads, bool print, double &a, double &b, double &c,
+                             int gpu_device = -1);
 
 int select_force_type(const Input &in);  // System.cpp:49-87
 std::string resolve_path(const std::string &json_path, const std::string &file);

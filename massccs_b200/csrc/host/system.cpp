@@ -90,8 +90,11 @@ SystemSetup::SystemSetup(const std::string &json_path, bool print)
 
   double t0 = now_s();
   if (in.equipotential_flag == 1) {  // System.cpp:120-126
+    // the rays' all-atom potentials on the GPU for large targets (setup_device)
+    const bool gpu = in.setup_device == "gpu" || (in.setup_device == "auto" && target.natoms >= 20000);
+    const int dev = gpu ? (in.devices.empty() ? 0 : in.devices[0]) : -1;
     equipotential_ellipsoid(target, g, in.polarizability_flag, in.temperatureTarget, mu, alpha,
-                            (int)std::max(1u, in.nthreads), print, a, b, c);
+                            (int)std::max(1u, in.nthreads), print, a, b, c, dev);
     if (print) std::cout << "ellipsoid axis length: " << a << "  " << b << "  " << c << "  Ang" << std::endl;
   } else {
     geometric_ellipsoid(print);

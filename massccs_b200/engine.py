@@ -107,7 +107,8 @@ EXPORTS = ["ccs_version", "ccs_create", "ccs_destroy", "ccs_params_default", "cc
            "ccs_eval_setup", "ccs_get_info", "ccs_status_string", "ccs_last_error",
            "ccs_measure_fp32_peak", "ccs_run_device_noalloc", "ccs_run_batch",
            "ccs_field_params_default", "ccs_field_train", "ccs_field_enable", "ccs_field_eval",
-           "ccs_field_setup", "ccs_field_get_weights", "ccs_field_set_weights", "ccs_field_loss_grad"]
+           "ccs_field_setup", "ccs_field_get_weights", "ccs_field_set_weights", "ccs_field_loss_grad",
+           "ccs_equipotential_points"]
 
 _LIB = None
 

@@ -16,12 +16,15 @@ feeding a two-hidden-layer ReLU MLP:
              (continuous first derivatives, so the forces of the field are
              continuous).  e(x): L * F features; J(x) = de/dx.
   MLP        z1 = W1 e + b1, a1 = relu(z1); z2 = W2 a1 + b2, a2 = relu(z2);
-             u_f = s (w3_f . a2 + b3_f) for each output field f (one per gas
-             site type), s a fixed output scale.
-  forces     F_f = -du_f/dx = -s J^T W1^T (m1 * W2^T (m2 * w3_f)), m = z > 0.
+             u_f = s_f (w3_f . a2 + b3_f) for each output field f, s_f a fixed
+             per-field output scale (the RMS of its labels).  The engine's
+             fields are the smooth far parts of its range-separated forces:
+             the far potential of each gas site type and, with the induced
+             dipole, the three components of the far electric field.
+  forces     F_f = -du_f/dx = -s_f J^T W1^T (m1 * W2^T (m2 * w3_f)), m = z > 0.
   loss       per sample, sum over fields of
-               lam_u (u_f - U*_f)^2 / (U*_f^2 + u0^2) + |F_f - F*_f|^2 / (|F*_f|^2 + f0^2)
-             (relative errors with floors), averaged over the batch.  Its
+               lam_u (u_f - U*_f)^2 / (U*_f^2 + u0_f^2) + |F_f - F*_f|^2 / (|F*_f|^2 + f0_f^2)
+             (relative errors with per-field floors), averaged over the batch.  Its
              parameter gradients pass twice through the network (the force
              is itself a gradient): `loss_and_grad`.
   inference  `infer_bf16`: the arithmetic of the tensor-core path -- table
@@ -109,6 +112,7 @@ class Field:
     """Hash-grid encoding + MLP with one potential output per field."""
 
     def __init__(self, lo, hi, hidden=64, outputs=2, scale=1.0, seed=0, **grid):
+        """scale: one output scale for every field, or a sequence of nf."""
         self.grid = HashGrid(lo, hi, seed=seed, **grid)
         rng = np.random.default_rng(seed + 1)
         E = self.grid.L * self.grid.F
@@ -118,7 +122,7 @@ class Field:
         self.b2 = np.zeros(hidden)
         self.W3 = rng.normal(0, np.sqrt(1.0 / hidden), size=(outputs, hidden))
         self.b3 = np.zeros(outputs)
-        self.s = float(scale)
+        self.s = np.broadcast_to(np.asarray(scale, dtype=np.float64), (outputs,)).copy()
 
     # parameters as a flat MLP vector in the GPU's order: W1, b1, W2, b2, W3, b3
     def mlp_vector(self):
@@ -147,15 +151,17 @@ class Field:
         g2 = m2[:, None, :] * self.W3[None, :, :]              # (n, nf, H)
         g1 = m1[:, None, :] * (g2 @ self.W2)                   # (n, nf, H): W2^T g2
         g0 = g1 @ self.W1                                      # (n, nf, E): W1^T g1
-        F = -self.s * np.einsum("nfe,nea->nfa", g0, J)
+        F = -self.s[None, :, None] * np.einsum("nfe,nea->nfa", g0, J)
         st = dict(e=e, J=J, cache=cache, z1=z1, m1=m1, a1=a1, z2=z2, m2=m2, a2=a2, g2=g2, g1=g1, g0=g0)
         return u, F, st
 
     def loss_and_grad(self, x, U, Fs, lam_u=0.1, u0=0.05, f0=0.05):
         """Mean loss over the batch and its gradients: (loss, dtable, dmlp vector).
-        U (n, nf), Fs (n, nf, 3) are the labels."""
+        U (n, nf), Fs (n, nf, 3) are the labels; u0, f0: floors (scalars or per field)."""
         n = x.shape[0]
         u, F, st = self.forward(x)
+        u0 = np.asarray(u0, dtype=np.float64)
+        f0 = np.asarray(f0, dtype=np.float64)
         wu = lam_u / (U * U + u0 * u0)                         # (n, nf)
         wf = 1.0 / ((Fs * Fs).sum(-1) + f0 * f0)               # (n, nf)
         du = u - U
@@ -166,9 +172,10 @@ class Field:
         du_ = 2.0 * wu * du / n                                # dL/du (n, nf)
         eF = 2.0 * wf[..., None] * dF / n                      # dL/dF (n, nf, 3)
         # ---- potential path
-        dW3 = s * du_.T @ a2
-        db3 = s * du_.sum(0)
-        da2 = s * du_ @ self.W3                                # (n, H)
+        sd = du_ * s[None, :]
+        dW3 = sd.T @ a2
+        db3 = sd.sum(0)
+        da2 = sd @ self.W3                                     # (n, H)
         dz2 = m2 * da2
         dW2 = dz2.T @ a1
         db2 = dz2.sum(0)
@@ -176,9 +183,9 @@ class Field:
         dW1 = dz1.T @ e
         db1 = dz1.sum(0)
         de = dz1 @ self.W1                                     # (n, E)
-        # ---- force path: F_f = -s J^T g0_f
-        r0 = -s * np.einsum("nea,nfa->nfe", J, eF)             # dL/dg0 (n, nf, E)
-        dJ = -s * np.einsum("nfe,nfa->nea", g0, eF)            # dL/dJ (n, E, 3)
+        # ---- force path: F_f = -s_f J^T g0_f
+        r0 = -s[None, :, None] * np.einsum("nea,nfa->nfe", J, eF)  # dL/dg0 (n, nf, E)
+        dJ = -np.einsum("nfe,nfa->nea", g0 * s[None, :, None], eF)  # dL/dJ (n, E, 3)
         dW1 += np.einsum("nfh,nfe->he", g1, r0)                # g0 = W1^T g1
         r1 = r0 @ self.W1.T                                    # dL/dg1 (n, nf, H)
         h = m1[:, None, :] * r1                                # through g1 = m1 * (W2^T g2)
@@ -212,8 +219,18 @@ class Field:
         G2 = bf16(m2[:, None, :] * W3[None, :, :])
         G1 = bf16(m1[:, None, :] * (G2 @ W2))
         g0 = G1 @ W1
-        F = -self.s * np.einsum("nfe,nea->nfa", g0, J)
+        F = -self.s[None, :, None] * np.einsum("nfe,nea->nfa", g0, J)
         return u, F
+
+
+def switch(r, r_in, r_out):
+    """The range-separation weight of a pair at distance r: 1 below r_in, 0
+    above r_out, the quintic smootherstep 1 - x^3 (10 - 15 x + 6 x^2) between
+    (x = (r - r_in) / (r_out - r_in)), and its derivative d/dr."""
+    x = np.clip((np.asarray(r, dtype=np.float64) - r_in) / (r_out - r_in), 0.0, 1.0)
+    S = 1.0 - x ** 3 * (10.0 - 15.0 * x + 6.0 * x * x)
+    dS = -30.0 * x * x * (1.0 - x) ** 2 / (r_out - r_in)
+    return S, dS
 
 
 def adam_step(p, g, m, v, t, lr, b1=0.9, b2=0.99, eps=1e-15):

@@ -12,7 +12,7 @@ import numpy as np
 
 def _field(seed=0, outputs=2):
     from oracle.surrogate import Field
-    f = Field(lo=[-5, -5, -5], hi=[5, 5, 5], hidden=16, outputs=outputs, scale=0.7, seed=seed,
+    f = Field(lo=[-5, -5, -5], hi=[5, 5, 5], hidden=16, outputs=outputs, scale=(0.7, 2.0)[:outputs], seed=seed,
               levels=4, log2_table=8, features=2, base=4, finest=32)
     rng = np.random.default_rng(seed + 10)
     f.grid.table = rng.normal(0, 0.5, size=f.grid.table.shape)  # away from the tiny initial values
