@@ -473,7 +473,7 @@ def run_field_bench(args, rank, world, local):
                       "gain_over_plain": plain_ms / field_ms},
             "training": {"wall_s": train_s, **{k: rep[k] for k in (
                 "samples", "sample_ms", "label_ms", "train_ms", "validate_ms", "first_loss", "final_loss",
-                "val_force_rel_rms", "val_force_rel_p99", "val_u_abs_rms", "exact_fraction", "err_voxels")}},
+                "val_force_rel_rms", "val_force_rel_p99", "val_u_rel_rms", "exact_fraction", "err_voxels")}},
             "e2e": {"value": world * n / e2e_s, "unit": "trajectories/s",
                     "h2d_bytes_per_step": 9 * 8 * n, "d2h_bytes_per_step": 9 * n,
                     "includes": "ccs_run with the learned field (H2D, both passes, D2H) and the reduction; "

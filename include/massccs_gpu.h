@@ -234,16 +234,21 @@ int ccs_measure_fp32_peak(int device, double ms, double *tflops);
 /* ---- Learned field ---------------------------------------------------------
  * No counterpart in the reference, which evaluates every force of every step
  * with the linked-cell sums (src/Force.cpp:34-1725); the learned field
- * replaces those sums where it is trusted.  Per context (target + gas): a
+ * replaces most of those sums.  Range separation: every pair term is split
+ * by a smooth switch S(r) (1 below r_in, 0 above r_out) into a near part,
+ * summed exactly over the atoms within r_out, and a far part, which is smooth
+ * in the site position and is learned.  Per context (target + gas): a
  * 16-level hash-grid encoding of the site position (2 features per level,
- * smoothstep blending) feeding an MLP 32 -> 64 -> 64 -> one potential per gas
- * site type; forces are minus its gradient (a conservative field).  It is
- * trained on the GPU (ccs_field_train: samples from the context's own exact
- * evaluator, the project's forward/backward and Adam kernels) and evaluated
- * in the lane pass by tcgen05 BF16 tensor-core MMAs with FP32 accumulation.
- * A position is evaluated exactly when it lies within fallback_radius of an
- * atom, outside the field's domain, or in a voxel whose validation error
- * exceeds err_threshold.  FP32 precision only. */
+ * smoothstep blending) feeding an MLP 32 -> 64 -> 64 -> nf fields: the far
+ * potential of each gas site type and, with the induced dipole, the three
+ * far-field components; far forces and the far field's Jacobian are minus the
+ * fields' gradients.  It is trained on the GPU (ccs_field_train: samples
+ * labelled by the engine's own cell grid and tables, the project's
+ * forward/backward and Adam kernels) and evaluated in the lane pass by
+ * tcgen05 BF16 tensor-core MMAs with FP32 accumulation.  A position is
+ * evaluated fully exactly when it lies within fallback_radius of an atom,
+ * outside the field's domain, or in a voxel whose validation error exceeds
+ * err_threshold.  FP32 precision, force types 2, 4 and 6. */
 typedef struct {
   int64_t samples;          /* training samples (default 4,000,000) */
   int32_t iterations;       /* Adam steps (default 4000) */
@@ -260,9 +265,11 @@ typedef struct {
   double near_fraction;     /* share of samples drawn in the shell around atoms (default 0.5) */
   double near_shell;        /* A: that shell's thickness beyond fallback_radius (default 6.0) */
   double lr;                /* Adam learning rate, decayed tenfold over the run (default 1e-2) */
-  double lam_u, u0, f0;     /* loss: lam_u (u-U*)^2/(U*^2+u0^2) + |F-F*|^2/(|F*|^2+f0^2)
-                               (defaults 0.1, 0.05 kcal/mol, 0.05 kcal/mol/A) */
+  double lam_u, u0, f0;     /* loss per field: lam_u (u-U*)^2/(U*^2+(u0 s)^2) + |G-G*|^2/(|G*|^2+(f0 g)^2),
+                               s and g the RMS of the field's values and gradients
+                               (defaults 0.1, 0.05, 0.05) */
   uint64_t seed;            /* sampling, initialisation and batch order (default 2104) */
+  double r_in, r_out;       /* A: the range-separation switch (defaults 6 and 8) */
 } ccs_field_params;
 
 typedef struct {
@@ -270,12 +277,14 @@ typedef struct {
   int32_t levels, dense_levels, nfields, log2_table;
   int32_t res[16];                    /* grid resolution per level */
   int64_t samples;                    /* training samples drawn */
-  double output_scale;                /* s: potentials are s * (network output) */
+  double output_scale[5];             /* per field: values are s_f * (network output) */
+  double gradient_scale[5];           /* per field: RMS of the gradient labels */
   double sample_ms, label_ms, train_ms, validate_ms;
   double first_loss, final_loss;      /* mean training loss of the first and last steps */
-  double val_force_rel_rms;           /* validation: RMS of |F - F*| / (|F*| + f0) */
+  double val_force_rel_rms;           /* validation: RMS over samples of the largest
+                                         |G - G*| / (|G*| + f0 g) of the fields */
   double val_force_rel_p99;
-  double val_u_abs_rms;               /* RMS |u - U*|, kcal/mol */
+  double val_u_rel_rms;               /* RMS of the largest |u - U*| / s of the fields */
   double exact_fraction;              /* share of the domain's voxels evaluated exactly */
   int64_t err_voxels;                 /* validation voxels above err_threshold */
 } ccs_field_report;
@@ -292,28 +301,36 @@ int ccs_field_train(ccs_ctx *ctx, const ccs_field_params *p, ccs_field_report *r
  * (on = 0, the default).  CCS_ERR_INVALID if no field is trained. */
 int ccs_field_enable(ccs_ctx *ctx, int on);
 
-/* Inference at npts positions (pos: npts x 3) for gas site `site`: u (npts),
- * f (npts x 3), and exact[i] = 1 where the trajectory kernels would evaluate
- * that position exactly (the field's values are still returned).  path 0:
- * the tensor-core kernel of the lane pass (128 positions per CTA); path 1:
- * the warp kernel of the warp pass.  exact may be NULL. */
-int ccs_field_eval(ccs_ctx *ctx, size_t npts, int site, const double *pos, int path, double *u, double *f,
-                   int8_t *exact);
+/* Inference of the fields gas site `site` uses (its far potential; at the
+ * dipole's site also the three far-field components: nfields = 1 or 4) at
+ * npts positions (pos: npts x 3): u (npts x 4: the values, nfields used),
+ * g (npts x 4 x 3: minus each field's gradient -- for a potential the far
+ * force), exact[i] = 1 where the trajectory kernels evaluate that position
+ * fully exactly (the field's values are still returned).  path 0: the
+ * tensor-core kernel of the lane pass (128 positions per CTA); path 1: the
+ * warp kernel of the warp pass.  exact and nfields may be NULL. */
+int ccs_field_eval(ccs_ctx *ctx, size_t npts, int site, const double *pos, int path, double *u, double *g,
+                   int8_t *exact, int32_t *nfields);
 
 /* Test hooks of the training kernels (the checker compares them with its
  * own restatement).  Parameters in FP32: table [16][2^log2_table][2], mlp =
- * W1 [64][32], b1 [64], W2 [64][64], b2 [64], W3 [nf][64], b3 [nf].
+ * W1 [64][32], b1 [64], W2 [64][64], b2 [64], W3 [nf][64], b3 [nf];
+ * scales: nf output scales, then nf gradient scales (the loss floors).
  * ccs_field_setup prepares a context's field geometry without training
  * (domain, grids, exact-evaluation bitmap) with random parameters;
  * ccs_field_get/set_weights read or replace the parameters (set also
  * refreshes the inference copies); ccs_field_loss_grad runs the training
  * forward/backward on n given samples (pos n x 3, labels n x nf x 4: U, Fx,
- * Fy, Fz) and returns the mean loss and its gradients. */
+ * Fy, Fz: a potential's force, i.e. minus the gradient) and returns the mean
+ * loss and its gradients. */
 int ccs_field_setup(ccs_ctx *ctx, const ccs_field_params *p, ccs_field_report *report);
-int ccs_field_get_weights(ccs_ctx *ctx, float *table, float *mlp, double *output_scale);
-int ccs_field_set_weights(ccs_ctx *ctx, const float *table, const float *mlp, double output_scale);
+int ccs_field_get_weights(ccs_ctx *ctx, float *table, float *mlp, double *scales);
+int ccs_field_set_weights(ccs_ctx *ctx, const float *table, const float *mlp, const double *scales);
 int ccs_field_loss_grad(ccs_ctx *ctx, size_t n, const float *pos, const float *labels, double *loss,
                         float *dtable, float *dmlp);
+/* The training labels at n positions: every field's far part and minus its
+ * gradient, labels n x nf x 4 (the engine's cell grid and FP32 tables). */
+int ccs_field_labels(ccs_ctx *ctx, size_t n, const double *pos, double *labels);
 
 /* The equipotential ellipsoid's boundary points on the GPU
  * (src/Equipotential.cpp:86-200 with the all-atom potentials of :203-557):

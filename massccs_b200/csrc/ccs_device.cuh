@@ -228,7 +228,12 @@ template <int G, typename T> __device__ __forceinline__ T group_sum(T v, unsigne
 // outside their cutoff are selected away (a select, never a multiply, so an
 // infinite or NaN term of an excluded pair cannot leak into the sums).  The
 // lanes of a warp therefore never diverge on a pair's distance.
-template <typename T, int GAS, bool HASQ>
+//
+// SPLIT: the near part of the learned field's range separation -- every term
+// weighted by the switch S(r) (field_device.cuh), its force by
+// -grad(S u) = S F - u S'(r) d / r, the dipole's field by S e and its
+// Jacobian by grad(S e) (still symmetric, since e is along d).
+template <typename T, int GAS, bool HASQ, bool SPLIT = false>
 __device__ __forceinline__ void visit_atom(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
                                            const bool (&act)[GasShape<GAS>::NS], const Atom<T> &a,
                                            Acc<T, GasShape<GAS>::NS> &acc) {
@@ -243,14 +248,25 @@ __device__ __forceinline__ void visit_atom(const KParams &kp, const T (&p)[GasSh
     const int lj = site_lj<GAS>(s);
     const T ir = Real<T>::rsq(r2);
     const T ir2 = ir * ir;
+    T sw = T(1), dsw = T(0);  // S and S'(r) / r
+    if constexpr (SPLIT) {
+      T dS;
+      range_switch(r2 * ir, T(kp.field.r_in), T(kp.field.r_out), sw, dS);
+      dsw = dS * ir;
+    }
     if (lj != 0) {
       // Force.cpp:83-102: U = A/r^12 - B/r^6 - (A/rc^12 - B/rc^6), F = (12A/r^12 - 6B/r^6)/r^2 * d
       const bool in_lj = r2 < rlj2;
       const T A = lj == 2 ? a.Ac : a.A, B = lj == 2 ? a.Bc : a.B;
       const T ir6 = ir2 * ir2 * ir2;
-      const T u = ir6 * (A * ir6 - B) - (A * T(kp.rc12inv) - B * T(kp.rc6inv));
-      const T fl = in_lj ? ir6 * (T(12) * A * ir6 - T(6) * B) * ir2 : T(0);
-      us += in_lj ? u : T(0);
+      const T u = in_lj ? ir6 * (A * ir6 - B) - (A * T(kp.rc12inv) - B * T(kp.rc6inv)) : T(0);
+      T fl = in_lj ? ir6 * (T(12) * A * ir6 - T(6) * B) * ir2 : T(0);
+      if constexpr (SPLIT) {
+        fl = sw * fl - u * dsw;
+        us += sw * u;
+      } else {
+        us += u;
+      }
       acc.f[s][0] += fl * dx; acc.f[s][1] += fl * dy; acc.f[s][2] += fl * dz;
     }
     if constexpr (HASQ) {
@@ -259,15 +275,24 @@ __device__ __forceinline__ void visit_atom(const KParams &kp, const T (&p)[GasSh
       if (site_coul<GAS>(s) && kp.coul_on) {
         // Force.cpp:671-683: U = k qi qj (1/r - 3/(2rc) + r^2/(2rc^3)), F = k qi qj (1/r^3 - 1/rc^3) d
         const T kq = T(KCOUL * kp.q_site[s]) * a.q;
-        const T u = kq * (ir - T(kp.c1) + T(kp.c2) * r2);
-        const T fc = in_c ? kq * (ir3 - T(kp.rc3inv)) : T(0);
-        us += in_c ? u : T(0);
+        const T u = in_c ? kq * (ir - T(kp.c1) + T(kp.c2) * r2) : T(0);
+        T fc = in_c ? kq * (ir3 - T(kp.rc3inv)) : T(0);
+        if constexpr (SPLIT) {
+          fc = sw * fc - u * dsw;
+          us += sw * u;
+        } else {
+          us += u;
+        }
         acc.f[s][0] += fc * dx; acc.f[s][1] += fc * dy; acc.f[s][2] += fc * dz;
       }
       if (s == GasShape<GAS>::DIP && kp.dip_on) {
         // Force.cpp:393-426: E += q (1/r^3 - 1/rc^3) d ; dE_ab += q (1/r^3 - 1/rc^3) delta_ab - 3 q d_a d_b / r^5
-        const T sq = in_c ? a.q * (ir3 - T(kp.rc3inv)) : T(0);
-        const T tq = in_c ? T(-3) * a.q * ir3 * ir2 : T(0);
+        T sq = in_c ? a.q * (ir3 - T(kp.rc3inv)) : T(0);
+        T tq = in_c ? T(-3) * a.q * ir3 * ir2 : T(0);
+        if constexpr (SPLIT) {  // E = S e, grad E = S grad e + (S'/r) e d^T
+          tq = sw * tq + sq * dsw;
+          sq = sw * sq;
+        }
         acc.E[0] += sq * dx; acc.E[1] += sq * dy; acc.E[2] += sq * dz;
         const T tx = tq * dx, ty = tq * dy;
         acc.G[0] += sq + tx * dx;
@@ -365,6 +390,41 @@ __device__ __forceinline__ void finish_row(const KParams &kp, const T *row, cons
     if (!act[s]) { f[s][0] = f[s][1] = f[s][2] = U[s] = T(0); }
 }
 
+// Site forces and energies of a learned-field step: the exact near sums of
+// the range separation (row, as finish_row reads it) plus the far parts --
+// per site its far potential ufar and force ffar; at the dipole site the
+// field E = E_near + E_far and its Jacobian J = J_near + J_far
+// (Jf[a][b] = d E_far_a / d x_b), giving the induced-dipole force
+// alpha J^T E and energy -alpha/2 |E|^2 (Force.cpp:483-487).
+template <typename T, int GAS, bool HASQ>
+__device__ __forceinline__ void finish_split(const KParams &kp, const T *row, const float (&ufar)[GasShape<GAS>::NS],
+                                             const float (&ffar)[GasShape<GAS>::NS][3], const float (&Ef)[3],
+                                             const float (&Jf)[3][3], const bool (&act)[GasShape<GAS>::NS],
+                                             T (&f)[GasShape<GAS>::NS][3], T (&U)[GasShape<GAS>::NS]) {
+  constexpr int NS = GasShape<GAS>::NS;
+#pragma unroll
+  for (int s = 0; s < NS; s++) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) f[s][k] = row[4 * s + k] + T(ffar[s][k]);
+    U[s] = row[4 * s + 3] + T(ufar[s]);
+  }
+  if (HASQ && kp.dip_on) {
+    constexpr int d = GasShape<GAS>::DIP;
+    const T al = T(kp.alpha);
+    const T *En = row + 4 * NS, *Gn = row + 4 * NS + 3;  // near E; near Jacobian xx yy zz xy xz yz
+    const T E[3] = {En[0] + T(Ef[0]), En[1] + T(Ef[1]), En[2] + T(Ef[2])};
+    const T Jt[3][3] = {{Gn[0] + T(Jf[0][0]), Gn[3] + T(Jf[0][1]), Gn[4] + T(Jf[0][2])},
+                        {Gn[3] + T(Jf[1][0]), Gn[1] + T(Jf[1][1]), Gn[5] + T(Jf[1][2])},
+                        {Gn[4] + T(Jf[2][0]), Gn[5] + T(Jf[2][1]), Gn[2] + T(Jf[2][2])}};
+#pragma unroll
+    for (int a = 0; a < 3; a++) f[d][a] += al * (E[0] * Jt[0][a] + E[1] * Jt[1][a] + E[2] * Jt[2][a]);
+    U[d] -= T(0.5) * al * (E[0] * E[0] + E[1] * E[1] + E[2] * E[2]);
+  }
+#pragma unroll
+  for (int s = 0; s < NS; s++)
+    if (!act[s]) { f[s][0] = f[s][1] = f[s][2] = U[s] = T(0); }
+}
+
 // Candidate visits of one probe configuration by a group of G lanes (G = 1:
 // one lane alone).  All lanes of the group call it with identical arguments;
 // each accumulates its share of the candidates into acc.
@@ -372,7 +432,7 @@ __device__ __forceinline__ void finish_row(const KParams &kp, const T *row, cons
 //   cen     centre of the sites, off: largest |p_s - cen|
 //   glist   the group's candidate buffer in shared memory, GCAP_PER_LANE * G ints
 constexpr int GCAP_PER_LANE = 8;
-template <typename T, int G, int GAS, bool HASQ>
+template <typename T, int G, int GAS, bool HASQ, bool SPLIT = false>
 __device__ __forceinline__ void accumulate_group(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
                                                  const bool (&act)[GasShape<GAS>::NS], const T (&cen)[3], T off,
                                                  Acc<T, GasShape<GAS>::NS> &acc, uint32_t &visits, int g,
@@ -385,7 +445,8 @@ __device__ __forceinline__ void accumulate_group(const KParams &kp, const T (&p)
   if (!any) return;
   uint32_t nvis = 0;
   // candidate sphere around the centre; +1e-3 A so rounding never drops a pair
-  const T R = kp.allpairs ? T(INFINITY) : T(kp.reach) + off + T(1e-3);
+  // (the near part of the range separation reaches r_out only)
+  const T R = kp.allpairs ? T(INFINITY) : (SPLIT ? T(kp.field.r_out) : T(kp.reach)) + off + T(1e-3);
   const T cx = cen[0], cy = cen[1], cz = cen[2];
   const T ex = fmax(fmax(T(kp.bb_lo[0]) - cx, cx - T(kp.bb_hi[0])), T(0));
   const T ey = fmax(fmax(T(kp.bb_lo[1]) - cy, cy - T(kp.bb_hi[1])), T(0));
@@ -398,7 +459,7 @@ __device__ __forceinline__ void accumulate_group(const KParams &kp, const T (&p)
     // atoms per lane of the group: every atom is a candidate
     for (int ai = g; ai < kp.natoms; ai += G) {
       const Atom<T> a = load_atom<T, GAS>(kp, ai);
-      visit_atom<T, GAS, HASQ>(kp, p, act, a, acc);
+      visit_atom<T, GAS, HASQ, SPLIT>(kp, p, act, a, acc);
     }
     if (G == 1 || g == 0) nvis += (uint32_t)kp.natoms;
   } else if (ex * ex + ey * ey + ez * ez <= R * R) {
@@ -412,7 +473,7 @@ __device__ __forceinline__ void accumulate_group(const KParams &kp, const T (&p)
         nvis += (uint32_t)len;
         for (int ai = b; ai < b + len; ai++) {
           const Atom<T> a = load_atom<T, GAS>(kp, ai);
-          visit_atom<T, GAS, HASQ>(kp, p, act, a, acc);
+          visit_atom<T, GAS, HASQ, SPLIT>(kp, p, act, a, acc);
         }
       } else {
         // flatten the G runs of this chunk into the group's list: exclusive scan of run lengths
@@ -431,7 +492,7 @@ __device__ __forceinline__ void accumulate_group(const KParams &kp, const T (&p)
           const int m = min(GCAP, total - cs);
           for (int t = g; t < m; t += G) {
             const Atom<T> a = load_atom<T, GAS>(kp, glist[t]);
-            visit_atom<T, GAS, HASQ>(kp, p, act, a, acc);
+            visit_atom<T, GAS, HASQ, SPLIT>(kp, p, act, a, acc);
           }
           __syncwarp(mask);  // the list is rewritten next
         }
@@ -548,7 +609,7 @@ __device__ __forceinline__ int block_excl_scan(int len, int lane, int w, int *sm
 
 // Visit candidates list[0..m) (list == nullptr: atoms 0..m): thread tid
 // takes t, t+NT, ... two per iteration for instruction-level parallelism.
-template <typename T, int NT, int GAS, bool HASQ>
+template <typename T, int NT, int GAS, bool HASQ, bool SPLIT = false>
 __device__ __forceinline__ void visit_list(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
                                            const bool (&act)[GasShape<GAS>::NS], const int *list, int m, int tid,
                                            Acc<T, GasShape<GAS>::NS> &acc) {
@@ -556,12 +617,12 @@ __device__ __forceinline__ void visit_list(const KParams &kp, const T (&p)[GasSh
   for (; t + NT < m; t += 2 * NT) {
     const Atom<T> a1 = load_atom<T, GAS>(kp, list ? list[t] : t);
     const Atom<T> a2 = load_atom<T, GAS>(kp, list ? list[t + NT] : t + NT);
-    visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
-    visit_atom<T, GAS, HASQ>(kp, p, act, a2, acc);
+    visit_atom<T, GAS, HASQ, SPLIT>(kp, p, act, a1, acc);
+    visit_atom<T, GAS, HASQ, SPLIT>(kp, p, act, a2, acc);
   }
   if (t < m) {
     const Atom<T> a1 = load_atom<T, GAS>(kp, list ? list[t] : t);
-    visit_atom<T, GAS, HASQ>(kp, p, act, a1, acc);
+    visit_atom<T, GAS, HASQ, SPLIT>(kp, p, act, a1, acc);
   }
 }
 
@@ -573,7 +634,7 @@ template <typename T, int GAS> struct ProbeSites {
   T p[GasShape<GAS>::NS][3];
   bool act[GasShape<GAS>::NS];
 };
-template <typename T, int NT, int GAS, bool HASQ>
+template <typename T, int NT, int GAS, bool HASQ, bool SPLIT = false>
 __device__ __noinline__ Acc<T, GasShape<GAS>::NS> chunked_visits(const KParams *__restrict__ kpg,
                                                                  const ProbeSites<T, GAS> ps, T cx, T cy, T cz,
                                                                  T R, int tid, int *sm_list, int *sm_wsum,
@@ -595,7 +656,7 @@ __device__ __noinline__ Acc<T, GasShape<GAS>::NS> chunked_visits(const KParams *
       const int lo = max(excl, cs), hi = min(excl + len, cs + LCAP);
       for (int q = lo; q < hi; q++) sm_list[q - cs] = b + (q - excl);
       __syncthreads();
-      visit_list<T, NT, GAS, HASQ>(kp, ps.p, ps.act, sm_list, min(LCAP, total - cs), tid, acc);
+      visit_list<T, NT, GAS, HASQ, SPLIT>(kp, ps.p, ps.act, sm_list, min(LCAP, total - cs), tid, acc);
       __syncthreads();  // the chunk is rewritten next
     }
     if (total == 0) __syncthreads();  // sm_wsum is rewritten next (block-uniform branch)
@@ -623,13 +684,17 @@ __device__ __noinline__ Acc<T, GasShape<GAS>::NS> chunked_visits(const KParams *
 // identical bits.  All threads call this with identical arguments.
 //   sm_list: LCAP ints; sm_wsum: NT/32 ints; sm_red: (NT/32 + 1) * RedShape<GAS>::P values
 //   list_n, list_c: the CTA's list state (list_n < 0: no valid list)
-template <typename T, int NT, int GAS, bool HASQ>
+//   SPLIT: the near part of the range separation (candidates within r_out);
+//   the raw sums (per site f and U, then E and its gradient) go to raw[] and
+//   the induced dipole is left to the caller, who adds the far parts first.
+template <typename T, int NT, int GAS, bool HASQ, bool SPLIT = false>
 __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p)[GasShape<GAS>::NS][3],
                                                   const bool (&act)[GasShape<GAS>::NS], const T (&cen)[3],
                                                   T off, T (&f)[GasShape<GAS>::NS][3],
                                                   T (&U)[GasShape<GAS>::NS], uint32_t &visits, int tid,
                                                   int *sm_list, int *sm_wsum, T *sm_red, int &list_n,
-                                                  T (&list_c)[3], const KParams *__restrict__ kpg) {
+                                                  T (&list_c)[3], const KParams *__restrict__ kpg,
+                                                  T *raw = nullptr) {
   constexpr int NS = GasShape<GAS>::NS;
   constexpr int NW = NT / 32;
   constexpr int NV = RedShape<GAS>::NV;
@@ -642,7 +707,7 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
   for (int s = 0; s < NS; s++) any |= act[s];
   uint32_t nvis = 0;
   if (any) {
-    const T R = kp.allpairs ? T(INFINITY) : T(kp.reach) + off + T(1e-3);
+    const T R = kp.allpairs ? T(INFINITY) : (SPLIT ? T(kp.field.r_out) : T(kp.reach)) + off + T(1e-3);
     const T cx = cen[0], cy = cen[1], cz = cen[2];
     const T ex = fmax(fmax(T(kp.bb_lo[0]) - cx, cx - T(kp.bb_hi[0])), T(0));
     const T ey = fmax(fmax(T(kp.bb_lo[1]) - cy, cy - T(kp.bb_hi[1])), T(0));
@@ -689,11 +754,11 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
           for (int k = 0; k < 3; k++) ps.p[s][k] = p[s][k];
         }
         uint32_t nc = 0;
-        acc = chunked_visits<T, NT, GAS, HASQ>(kpg, ps, cx, cy, cz, R, tid, sm_list, sm_wsum, &nc);
+        acc = chunked_visits<T, NT, GAS, HASQ, SPLIT>(kpg, ps, cx, cy, cz, R, tid, sm_list, sm_wsum, &nc);
         nvis += nc;
       }
     }
-    visit_list<T, NT, GAS, HASQ>(kp, p, act, lst, m, tid, acc);
+    visit_list<T, NT, GAS, HASQ, SPLIT>(kp, p, act, lst, m, tid, acc);
     nvis += (uint32_t)m;
   }
   // reduce-scatter per warp, then the warps in a fixed order
@@ -727,6 +792,12 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
   } else {
 #pragma unroll
     for (int k = 0; k < NV; k++) out[k] = __shfl_sync(0xffffffffu, v[0], k << SH);
+  }
+  if constexpr (SPLIT) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) raw[k] = out[k];
+    visits += nvis;
+    return;
   }
 #pragma unroll
   for (int s = 0; s < NS; s++) {
@@ -1317,13 +1388,14 @@ __global__ void __launch_bounds__(BLOCK, SURR ? 2 : CCS_LANE_MIN_BLOCKS)
             if ((actbits >> s) & 1u) surr &= !field_exact(kp.field, (float)p[s][0], (float)p[s][1], (float)p[s][2]);
         }
       }
-      if (near && !surr) {
+      if (near) {
         if constexpr (G == 1) {
           bool act[NS];
 #pragma unroll
           for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
-          eval_forces<T, 1, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis, 0,
-                                       1u << lane, nullptr);
+          if (!surr)
+            eval_forces<T, 1, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis, 0,
+                                         1u << lane, nullptr);
         } else {
 #pragma unroll
           for (int s = 0; s < NS; s++)
@@ -1368,21 +1440,80 @@ __global__ void __launch_bounds__(BLOCK, SURR ? 2 : CCS_LANE_MIN_BLOCKS)
       }
     }
     if constexpr (SURR) {
-      // the learned field for every probe outside the exact zone: one MLP tile
-      // of the CTA's 128 lanes per site
+      // the learned field for every probe outside the exact zone: the
+      // switched exact sums over the atoms within r_out ...
+      bool act[NS];
+#pragma unroll
+      for (int s = 0; s < NS; s++) act[s] = (actbits >> s) & 1u;
+      T raw[NV];
+      if constexpr (G == 1) {
+        if (surr) {
+          Acc<T, NS> acc;
+          acc.zero();
+          uint32_t nv = 0;
+          accumulate_group<T, 1, GAS, HASQ, true>(K, p, act, p[S::cs], site_offset<T, GAS>(p), acc, nv, 0, 1u << lane,
+                                                  nullptr);
+#pragma unroll
+          for (int k = 0; k < NV; k++) raw[k] = acc_value(acc, k);
+          L.nvis += nv;
+        }
+      } else {
+        __syncwarp();
+        const unsigned bal2 = __ballot_sync(FULL, surr);
+        const int n2 = __popc(bal2);
+        for (int idx = sub; idx < n2; idx += NSUB) {
+          const int t = wbase + nth_set_bit(bal2, idx);
+          T P[NS][3];
+          bool at[NS];
+          const unsigned ab = sm_act[t];
+#pragma unroll
+          for (int s = 0; s < NS; s++) {
+            at[s] = (ab >> s) & 1u;
+#pragma unroll
+            for (int k = 0; k < 3; k++) P[s][k] = sm_pos[t][s][k];
+          }
+          uint32_t nv = 0;
+          Acc<T, NS> acc;
+          acc.zero();
+          accumulate_group<T, G, GAS, HASQ, true>(kp, P, at, P[S::cs], site_offset<T, GAS>(P), acc, nv, g, gmask,
+                                                  sm_glist + (wbase + sub * G) * GCAP_PER_LANE);
+          reduce_group_row<T, G, GAS>(acc, g, gmask, sm_row[t]);
+          if (g == 0) sm_vis[t] = nv;
+        }
+        __syncwarp();
+        if (surr) {
+#pragma unroll
+          for (int k = 0; k < NV; k++) raw[k] = sm_row[threadIdx.x][k];
+          L.nvis += sm_vis[threadIdx.x];
+        }
+      }
+      // ... plus the far parts from the network: one MLP tile of the CTA's
+      // 128 lanes per site (the dipole's site also gives the far field)
+      float ufar[NS], ffar[NS][3], Ef[3] = {0.f, 0.f, 0.f}, Jf[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+#pragma unroll
+      for (int s = 0; s < NS; s++) { ufar[s] = 0.f; ffar[s][0] = ffar[s][1] = ffar[s][2] = 0.f; }
       if (__syncthreads_or(surr)) {
         bool ok = true;
 #pragma unroll 1
         for (int s = 0; s < NS && ok; s++) {
-          const bool use = surr && ((actbits >> s) & 1u);
+          const bool use = surr && act[s];
           float x[3] = {0.f, 0.f, 0.f};
           if (use) { x[0] = (float)p[s][0]; x[1] = (float)p[s][1]; x[2] = (float)p[s][2]; }
-          float e[FL_E], J[FL_E][3], u, f3[3];
+          int fl[FL_SITE_FIELDS];
+          const int nfo = site_fields(kp.field, s, fl);
+          float e[FL_E], J[FL_E][3], u[FL_SITE_FIELDS], gr[FL_SITE_FIELDS][3];
           field_encode(kp.field, x, e, J);
-          ok = tc_site(kp.field, tc_smem, tmem, tc_phase, use, e, J, kp.field.site_field[s], u, f3);
-          if (surr) {
-            fs[s][0] = use ? f3[0] : 0.f; fs[s][1] = use ? f3[1] : 0.f; fs[s][2] = use ? f3[2] : 0.f;
-            Us[s] = use ? u : 0.f;
+          ok = tc_site(kp.field, tc_smem, tmem, tc_phase, use, e, J, nfo, fl, u, gr);
+          if (use) {
+            ufar[s] = u[0];
+            ffar[s][0] = gr[0][0]; ffar[s][1] = gr[0][1]; ffar[s][2] = gr[0][2];
+            if (nfo == 4)
+#pragma unroll
+              for (int a = 0; a < 3; a++) {
+                Ef[a] = u[1 + a];
+#pragma unroll
+                for (int b = 0; b < 3; b++) Jf[a][b] = -gr[1 + a][b];
+              }
           }
         }
         if (!ok) {  // a tensor-core stage never completed (uniform): stop the kernel
@@ -1391,6 +1522,7 @@ __global__ void __launch_bounds__(BLOCK, SURR ? 2 : CCS_LANE_MIN_BLOCKS)
           break;
         }
       }
+      if (surr) finish_split<T, GAS, HASQ>(K, raw, ufar, ffar, Ef, Jf, act, fs, Us);
     }
     if (L.mode == M_IDLE) continue;
     if (!near) {
@@ -1467,7 +1599,7 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
   using S = Sites<GAS>;
   constexpr int NS = S::NS;
   static_assert(!SURR || (sizeof(T) == 4 && !BATCH), "the learned field runs in FP32 single-ion launches");
-  __shared__ float sm_site[NS][4];
+  __shared__ float sm_site[NS][4 * FL_SITE_FIELDS];
   __shared__ int sm_list[LCAP], sm_wsum[NT / 32];
   __shared__ T sm_red[(NT / 32 + 1) * RedShape<GAS>::P];
   __shared__ unsigned long long blk[8];
@@ -1521,6 +1653,7 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
     const KParams &K = ion_params<BATCH>(kp, L.ion);
     const KParams *Kg = ion_params_ptr<BATCH>(kp, kpg, L.ion);
     int list_n = -1;  // this trajectory's candidate list (none yet)
+    int list_split = -1;  // with the learned field: the list's mode (1: near part of the range separation)
     T list_c[3] = {T(0), T(0), T(0)};
     for (unsigned it = 1;; it++) {
       int r = S_CONTINUE;
@@ -1552,21 +1685,48 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
               if (act[s]) surr &= !field_exact(kp.field, (float)p[s][0], (float)p[s][1], (float)p[s][2]);
           }
           if (surr) {
-            for (int s = tid >> 5; s < NS; s += NT / 32) {
-              float u = 0.f, f3[3] = {0.f, 0.f, 0.f};
-              if (act[s]) {
-                const float x[3] = {(float)p[s][0], (float)p[s][1], (float)p[s][2]};
-                field_site_warp(kp.field, x, kp.field.site_field[s], u, f3);
+            if constexpr (SURR) {
+              // the switched exact sums over the atoms within r_out ...
+              T raw[RedShape<GAS>::NV];
+              if (list_split != 1) { list_n = -1; list_split = 1; }  // the candidate list has this mode's reach
+              eval_forces_block<T, NT, GAS, HASQ, true>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
+                                                        tid, sm_list, sm_wsum, sm_red, list_n, list_c, Kg, raw);
+              // ... plus the far parts from the network, one warp per site
+              for (int s = tid >> 5; s < NS; s += NT / 32) {
+                int fl[FL_SITE_FIELDS];
+                const int nfo = site_fields(kp.field, s, fl);
+                float u[FL_SITE_FIELDS] = {0.f, 0.f, 0.f, 0.f}, gr[FL_SITE_FIELDS][3] = {};
+                if (act[s]) {
+                  const float x[3] = {(float)p[s][0], (float)p[s][1], (float)p[s][2]};
+                  field_site_warp(kp.field, x, nfo, fl, u, gr);
+                }
+                if ((tid & 31) == 0)
+                  for (int k = 0; k < FL_SITE_FIELDS; k++) {
+                    sm_site[s][4 * k] = u[k];
+                    sm_site[s][4 * k + 1] = gr[k][0]; sm_site[s][4 * k + 2] = gr[k][1]; sm_site[s][4 * k + 3] = gr[k][2];
+                  }
               }
-              if ((tid & 31) == 0) { sm_site[s][0] = f3[0]; sm_site[s][1] = f3[1]; sm_site[s][2] = f3[2]; sm_site[s][3] = u; }
+              __syncthreads();
+              float ufar[NS], ffar[NS][3], Ef[3] = {0.f, 0.f, 0.f}, Jf[3][3];
+  #pragma unroll
+              for (int s = 0; s < NS; s++) {
+                ufar[s] = sm_site[s][0];
+                ffar[s][0] = sm_site[s][1]; ffar[s][1] = sm_site[s][2]; ffar[s][2] = sm_site[s][3];
+              }
+              const int ds = kp.field.dip_site;
+  #pragma unroll
+              for (int a = 0; a < 3; a++) {
+                Ef[a] = ds >= 0 ? sm_site[ds < NS ? ds : 0][4 * (1 + a)] : 0.f;
+  #pragma unroll
+                for (int b = 0; b < 3; b++) Jf[a][b] = ds >= 0 ? -sm_site[ds < NS ? ds : 0][4 * (1 + a) + 1 + b] : 0.f;
+              }
+              __syncthreads();
+              finish_split<T, GAS, HASQ>(K, raw, ufar, ffar, Ef, Jf, act, fs, Us);
             }
-            __syncthreads();
-#pragma unroll
-            for (int s = 0; s < NS; s++) {
-              fs[s][0] = T(sm_site[s][0]); fs[s][1] = T(sm_site[s][1]); fs[s][2] = T(sm_site[s][2]); Us[s] = T(sm_site[s][3]);
-            }
-            __syncthreads();
           } else {
+            if constexpr (SURR) {
+              if (list_split != 0) { list_n = -1; list_split = 0; }
+            }
             eval_forces_block<T, NT, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
                                                   tid, sm_list, sm_wsum, sm_red, list_n, list_c, Kg);
           }

@@ -4,9 +4,10 @@
 // ccs_field_* entry points of include/massccs_gpu.h.
 //
 // No counterpart in the reference (cces-cepid/massccs): its trajectory loop
-// evaluates every force exactly (src/Force.cpp:34-1725).  The labels come from
-// this engine's own exact evaluator (force_points_kernel, the same code as the
-// trajectory kernels), so the field learns exactly the forces it replaces.
+// evaluates every force exactly (src/Force.cpp:34-1725).  The network learns
+// the far part of the range-separated pair terms (field_device.cuh): the
+// labels are those terms weighted by 1 - S(r), summed over the target's atoms
+// within the cutoffs with this engine's own cell grid and parameter tables.
 //
 // Training is deterministic for a given seed: samples and batches come from a
 // counter-based hash, the weight gradients from a fixed-order reduction, and
@@ -29,7 +30,7 @@ using namespace ccs_internal;
 
 namespace {
 
-// Master MLP vector (FP32): W1 [64][32], b1 [64], W2 [64][64], b2 [64], W3 [2][64], b3 [2].
+// Master MLP vector (FP32): W1 [64][32], b1 [64], W2 [64][64], b2 [64], W3 [5][64], b3 [5].
 constexpr int MO_W1 = 0;
 constexpr int MO_B1 = MO_W1 + FL_H * FL_E;
 constexpr int MO_W2 = MO_B1 + FL_H;
@@ -46,6 +47,18 @@ struct TrainGeo {
   int dense[FL_LEVELS];
   uint32_t tmask;
   int log2t;
+  float s[FL_NF];        // output scales
+  float u0[FL_NF], f0[FL_NF];  // loss floors of each field's value and gradient
+};
+
+// What a field is, for its labels: the far potential of a gas site type
+// (LJ parameter set lj: 0 none, 1 primary, 2 carbon; charge q) or component
+// a of the far electric field.
+struct FieldKind {
+  int kind[FL_NF];   // 0 potential, 1 field component
+  int lj[FL_NF];
+  double q[FL_NF];
+  int comp[FL_NF];
 };
 
 uint64_t mix64(uint64_t x) {  // splitmix64 finaliser (host)
@@ -59,10 +72,12 @@ uint64_t mix64(uint64_t x) {  // splitmix64 finaliser (host)
 
 struct FieldState {
   ccs_field_params p{};
-  int nf = 1, site_field[3] = {0, 0, 0}, rep_site[FL_NF] = {0, 0};
+  int nf = 1, site_field[3] = {0, 0, 0}, dip_site = -1, efield = 0;
+  FieldKind kinds{};
   FieldK k{};
   TrainGeo geo{};
-  double lo[3] = {0, 0, 0}, side = 0, s = 1.0;
+  double lo[3] = {0, 0, 0}, side = 0;
+  double s[FL_NF] = {1, 1, 1, 1, 1}, gs[FL_NF] = {1, 1, 1, 1, 1};  // output and gradient scales
   size_t rows = 0;  // table rows per level
   size_t nwords = 0;
   // parameters and optimiser state
@@ -150,19 +165,79 @@ __global__ void sample_kernel(uint64_t seed, uint64_t first, size_t n, const flo
   keep[i] = field_exact(F, x, y, z) ? 0 : 1;
 }
 
-__global__ void pos_to_double_kernel(const float4 *__restrict__ p, size_t n, double *out) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float4 v = p[i];
-  out[3 * i] = v.x; out[3 * i + 1] = v.y; out[3 * i + 2] = v.z;
-}
-
-__global__ void pack_labels_kernel(const double *__restrict__ f, const double *__restrict__ U, size_t n, int field,
-                                   int nf, float *lab) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float *o = lab + (i * nf + field) * 4;
-  o[0] = (float)U[i]; o[1] = (float)f[3 * i]; o[2] = (float)f[3 * i + 1]; o[3] = (float)f[3 * i + 2];
+// Far-part labels (value and minus the gradient of every field) at n
+// points: one warp per point, lanes over the (x, y) columns of the cell grid
+// that meet the reach sphere, FP64 sums of the FP32 pair terms.
+__global__ void __launch_bounds__(256) far_label_kernel(KParams kp, FieldKind fk, int nf, size_t n,
+                                                        const float4 *__restrict__ pos, float *lab) {
+  const int lane = threadIdx.x & 31;
+  const size_t w = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const float rin = kp.field.r_in, rout = kp.field.r_out;
+  const float rlj2 = (float)kp.rlj2, rc2 = (float)kp.rc2;
+  for (size_t i = w; i < n; i += nw) {
+    const float4 P = pos[i];
+    double acc[FL_NF][4];
+#pragma unroll
+    for (int f = 0; f < FL_NF; f++) acc[f][0] = acc[f][1] = acc[f][2] = acc[f][3] = 0.0;
+    const float R = (float)kp.reach + 1e-3f;
+    int i0, j0, nj;
+    float inv_nj;
+    const int ncol = column_range<float>(kp, P.x, P.y, R, i0, j0, nj, inv_nj);
+    for (int c = lane; c < ncol; c += 32) {
+      int b, len;
+      column_run<float>(kp, c, ncol, i0, j0, nj, inv_nj, P.x, P.y, P.z, R, b, len);
+      for (int ai = b; ai < b + len; ai++) {
+        const float4 a = __ldg(&kp.xyzq32[ai]);
+        const float dx = P.x - a.x, dy = P.y - a.y, dz = P.z - a.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float ir = rsqrtf(r2), ir2 = ir * ir, ir3 = ir * ir2;
+        float S, dS;
+        range_switch(r2 * ir, rin, rout, S, dS);
+        const float wf = 1.f - S, dsr = dS * ir;  // far weight; S'(r) / r
+        const bool in_lj = r2 < rlj2, in_c = r2 < rc2;
+        for (int f = 0; f < nf; f++) {
+          if (fk.kind[f] == 0) {  // far potential: (1 - S) u, force (1 - S) F + u S' d / r
+            float u = 0.f, fs = 0.f;
+            if (fk.lj[f]) {
+              const float2 ab = __ldg(fk.lj[f] == 2 ? &kp.abc32[ai] : &kp.ab32[ai]);
+              const float ir6 = ir2 * ir2 * ir2;
+              if (in_lj) {
+                u += ir6 * (ab.x * ir6 - ab.y) - (ab.x * (float)kp.rc12inv - ab.y * (float)kp.rc6inv);
+                fs += ir6 * (12.f * ab.x * ir6 - 6.f * ab.y) * ir2;
+              }
+            }
+            if (fk.q[f] != 0.0 && kp.coul_on && in_c) {
+              const float kq = (float)(KCOUL * fk.q[f]) * a.w;
+              u += kq * (ir - (float)kp.c1 + (float)kp.c2 * r2);
+              fs += kq * (ir3 - (float)kp.rc3inv);
+            }
+            const float fsc = wf * fs + u * dsr;
+            acc[f][0] += (double)(wf * u);
+            acc[f][1] += (double)(fsc * dx); acc[f][2] += (double)(fsc * dy); acc[f][3] += (double)(fsc * dz);
+          } else if (in_c) {  // far field component a: (1 - S) e_a, minus its gradient
+            const int ca = fk.comp[f];
+            const float sq = a.w * (ir3 - (float)kp.rc3inv), tq = -3.f * a.w * ir3 * ir2;
+            const float d[3] = {dx, dy, dz};
+            acc[f][0] += (double)(wf * sq * d[ca]);
+            // grad (1 - S) e_a = (1 - S)(sq delta_a + tq d_a d) - sq d_a (S'/r) d
+            const float t2 = wf * tq * d[ca] - sq * d[ca] * dsr;
+#pragma unroll
+            for (int b = 0; b < 3; b++) acc[f][1 + b] -= (double)(t2 * d[b] + (b == ca ? wf * sq : 0.f));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < FL_NF; f++)
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[f][k] += __shfl_xor_sync(0xffffffffu, acc[f][k], o);
+    if (lane == 0)
+      for (int f = 0; f < nf; f++)
+        for (int k = 0; k < 4; k++) lab[(i * nf + f) * 4 + k] = (float)acc[f][k];
+  }
 }
 
 // batch indices of a training step (with replacement, counter-based)
@@ -180,9 +255,9 @@ __global__ void batch_kernel(uint64_t seed, uint64_t step, int B, size_t n, int 
 // the sample's loss, and adds the table gradients (fixed point).
 template <int NF>
 __global__ void __launch_bounds__(256) train_kernel(const float2 *__restrict__ table, const float *__restrict__ mlp,
-                                                    TrainGeo G, float s, const float4 *__restrict__ pos,
+                                                    TrainGeo G, const float4 *__restrict__ pos,
                                                     const float *__restrict__ lab, const int *__restrict__ bidx,
-                                                    int B, float lam_u, float u0, float f0, float invB, float *L1,
+                                                    int B, float lam_u, float invB, float *L1,
                                                     float *R1, float *L2, float *R2, float *V3, float *lossbuf,
                                                     unsigned long long *tgrad) {
   constexpr int P = 1 + NF;
@@ -289,7 +364,7 @@ __global__ void __launch_bounds__(256) train_kernel(const float2 *__restrict__ t
       float up = sw3[f * FL_H + u0i] * a2a + sw3[f * FL_H + u1i] * a2b;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) up += __shfl_xor_sync(FULL, up, o);
-      const float u = s * (up + sb3[f]);
+      const float u = G.s[f] * (up + sb3[f]);
       g2a[f] = m2a ? sw3[f * FL_H + u0i] : 0.f;
       g2b[f] = m2b ? sw3[f * FL_H + u1i] : 0.f;
       float ga = 0.f, gb = 0.f;
@@ -314,14 +389,14 @@ __global__ void __launch_bounds__(256) train_kernel(const float2 *__restrict__ t
         for (int a = 0; a < 3; a++) Fv[a] += __shfl_xor_sync(FULL, Fv[a], o);
       }
       const float U = lb[4 * f], Fs[3] = {lb[4 * f + 1], lb[4 * f + 2], lb[4 * f + 3]};
-      const float wu = lam_u / (U * U + u0 * u0);
-      const float wf = 1.f / (Fs[0] * Fs[0] + Fs[1] * Fs[1] + Fs[2] * Fs[2] + f0 * f0);
+      const float wu = lam_u / (U * U + G.u0[f] * G.u0[f]);
+      const float wf = 1.f / (Fs[0] * Fs[0] + Fs[1] * Fs[1] + Fs[2] * Fs[2] + G.f0[f] * G.f0[f]);
       const float d = u - U;
       du[f] = 2.f * wu * d * invB;
       float fl = 0.f;
 #pragma unroll
       for (int a = 0; a < 3; a++) {
-        const float dF = -s * Fv[a] - Fs[a];
+        const float dF = -G.s[f] * Fv[a] - Fs[a];
         eF[f][a] = 2.f * wf * dF * invB;
         fl += dF * dF;
       }
@@ -330,7 +405,10 @@ __global__ void __launch_bounds__(256) train_kernel(const float2 *__restrict__ t
     // ---- potential path backward
     float da2a = 0.f, da2b = 0.f;
 #pragma unroll
-    for (int f = 0; f < NF; f++) { da2a += s * du[f] * sw3[f * FL_H + u0i]; da2b += s * du[f] * sw3[f * FL_H + u1i]; }
+    for (int f = 0; f < NF; f++) {
+      da2a += G.s[f] * du[f] * sw3[f * FL_H + u0i];
+      da2b += G.s[f] * du[f] * sw3[f * FL_H + u1i];
+    }
     const float dz2a = m2a ? da2a : 0.f, dz2b = m2b ? da2b : 0.f;
     float da1a = 0.f, da1b = 0.f;
 #pragma unroll 8
@@ -354,9 +432,9 @@ __global__ void __launch_bounds__(256) train_kernel(const float2 *__restrict__ t
     float dJ[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int f = 0; f < NF; f++) {
-      const float r0 = -s * (Jk[0] * eF[f][0] + Jk[1] * eF[f][1] + Jk[2] * eF[f][2]);
+      const float r0 = -G.s[f] * (Jk[0] * eF[f][0] + Jk[1] * eF[f][1] + Jk[2] * eF[f][2]);
 #pragma unroll
-      for (int a = 0; a < 3; a++) dJ[a] += -s * g0[f] * eF[f][a];
+      for (int a = 0; a < 3; a++) dJ[a] += -G.s[f] * g0[f] * eF[f][a];
       float r1a = 0.f, r1b = 0.f;
 #pragma unroll 8
       for (int k = 0; k < FL_E; k++) {
@@ -376,9 +454,9 @@ __global__ void __launch_bounds__(256) train_kernel(const float2 *__restrict__ t
       reinterpret_cast<float2 *>(L2 + rf * FL_H)[lane] = make_float2(g2a[f], g2b[f]);
       reinterpret_cast<float2 *>(R2 + rf * FL_H)[lane] = make_float2(ha, hb);
       float *v3 = V3 + ((size_t)j * NF + f) * (FL_H + 1);
-      v3[u0i] = s * du[f] * a2a + (m2a ? r2a : 0.f);
-      v3[u1i] = s * du[f] * a2b + (m2b ? r2b : 0.f);
-      if (lane == 0) v3[FL_H] = s * du[f];
+      v3[u0i] = G.s[f] * du[f] * a2a + (m2a ? r2a : 0.f);
+      v3[u1i] = G.s[f] * du[f] * a2b + (m2b ? r2b : 0.f);
+      if (lane == 0) v3[FL_H] = G.s[f] * du[f];
     }
     if (lane == 0) lossbuf[j] = loss * invB;
     // ---- table gradients of this lane's 4 corners, both features of its level
@@ -511,6 +589,9 @@ __global__ void adam_table_kernel(float2 *p, float2 *m, float2 *v, unsigned long
 }
 
 // ---- inference copies -------------------------------------------------------
+struct FieldScales {
+  float s[FL_NF];
+};
 __device__ __forceinline__ float bf16_rne(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
 
 __global__ void table_to_bf16_kernel(const float2 *__restrict__ t, size_t n, uint32_t *out) {
@@ -521,7 +602,7 @@ __global__ void table_to_bf16_kernel(const float2 *__restrict__ t, size_t n, uin
 }
 
 // FP32 inference copies and the tcgen05 B images from the master MLP (one CTA).
-__global__ void pack_mlp_kernel(const float *__restrict__ m, int nf, float *inf, uint16_t *umma) {
+__global__ void pack_mlp_kernel(const float *__restrict__ m, int nf, FieldScales sc, float *inf, uint16_t *umma) {
   for (int t = threadIdx.x; t < FL_H * FL_E; t += blockDim.x) {
     const int i = t / FL_E, k = t % FL_E;
     const float w = bf16_rne(m[MO_W1 + t]);
@@ -539,7 +620,10 @@ __global__ void pack_mlp_kernel(const float *__restrict__ m, int nf, float *inf,
     inf[FO_B2 + t] = m[MO_B2 + t];
   }
   for (int t = threadIdx.x; t < FL_NF * FL_H; t += blockDim.x) inf[FO_W3 + t] = (t / FL_H) < nf ? m[MO_W3 + t] : 0.f;
-  if (threadIdx.x < FL_NF) inf[FO_B3 + threadIdx.x] = (int)threadIdx.x < nf ? m[MO_B3 + threadIdx.x] : 0.f;
+  if (threadIdx.x < FL_NF) {
+    inf[FO_B3 + threadIdx.x] = (int)threadIdx.x < nf ? m[MO_B3 + threadIdx.x] : 0.f;
+    inf[FO_S + threadIdx.x] = sc.s[threadIdx.x];
+  }
   // B images, element (n, k) at (k / 8) * (N * 8) + n * 8 + (k % 8) (in bf16 units)
   auto put = [&](int base_bytes, int N, int n, int k, float v) {
     umma[base_bytes / 2 + (k / 8) * (N * 8) + n * 8 + (k % 8)] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
@@ -559,20 +643,25 @@ __global__ void pack_mlp_kernel(const float *__restrict__ m, int nf, float *inf,
 }
 
 // ---- inference kernels (validation and ccs_field_eval) ----------------------
-// Warp path: one warp per (position, field); u and F as doubles.
-__global__ void eval_warp_kernel(FieldK F, size_t n, const float4 *__restrict__ pos, int field, double *u,
-                                 double *f, int8_t *exact) {
+// Warp path: one warp per position; the site's fields (value and minus the
+// gradient, 4 slots per position) as doubles.
+__global__ void eval_warp_kernel(FieldK F, size_t n, const float4 *__restrict__ pos, int site, double *u,
+                                 double *g, int8_t *exact) {
   const size_t w = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
+  int fl[FL_SITE_FIELDS];
+  const int nfo = site_fields(F, site, fl);
   for (size_t i = w; i < n; i += nw) {
     const float4 p = pos[i];
     const float x[3] = {p.x, p.y, p.z};
-    float uu, ff[3];
-    field_site_warp(F, x, field, uu, ff);
+    float uu[FL_SITE_FIELDS], gg[FL_SITE_FIELDS][3];
+    field_site_warp(F, x, nfo, fl, uu, gg);
     if (lane == 0) {
-      u[i] = uu;
-      f[3 * i] = ff[0]; f[3 * i + 1] = ff[1]; f[3 * i + 2] = ff[2];
+      for (int k = 0; k < nfo; k++) {
+        u[4 * i + k] = uu[k];
+        for (int a = 0; a < 3; a++) g[(4 * i + k) * 3 + a] = gg[k][a];
+      }
       if (exact) exact[i] = field_exact(F, x[0], x[1], x[2]) ? 1 : 0;
     }
   }
@@ -580,11 +669,13 @@ __global__ void eval_warp_kernel(FieldK F, size_t n, const float4 *__restrict__ 
 
 // Tensor-core path: 128 positions per tile, CTAs stride over tiles.
 __global__ void __launch_bounds__(TC_ROWS) eval_tc_kernel(FieldK F, size_t n, const float4 *__restrict__ pos,
-                                                          int field, double *u, double *f, int8_t *exact,
+                                                          int site, double *u, double *g, int8_t *exact,
                                                           int *error) {
   extern __shared__ __align__(1024) unsigned char dsm[];
   const uint32_t tmem = tc_setup(F, dsm);
   uint32_t phase = 0;
+  int fl[FL_SITE_FIELDS];
+  const int nfo = site_fields(F, site, fl);
   const size_t ntiles = (n + TC_ROWS - 1) / TC_ROWS;
   for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const size_t i = tile * TC_ROWS + threadIdx.x;
@@ -596,14 +687,16 @@ __global__ void __launch_bounds__(TC_ROWS) eval_tc_kernel(FieldK F, size_t n, co
     }
     float e[FL_E], J[FL_E][3];
     field_encode(F, x, e, J);
-    float uu = 0.f, ff[3] = {0.f, 0.f, 0.f};
-    if (!tc_site(F, dsm, tmem, phase, use, e, J, field, uu, ff)) {
+    float uu[FL_SITE_FIELDS], gg[FL_SITE_FIELDS][3];
+    if (!tc_site(F, dsm, tmem, phase, use, e, J, nfo, fl, uu, gg)) {
       if (threadIdx.x == 0) atomicExch(error, 2);
       break;
     }
     if (use) {
-      u[i] = uu;
-      f[3 * i] = ff[0]; f[3 * i + 1] = ff[1]; f[3 * i + 2] = ff[2];
+      for (int k = 0; k < nfo; k++) {
+        u[4 * i + k] = uu[k];
+        for (int a = 0; a < 3; a++) g[(4 * i + k) * 3 + a] = gg[k][a];
+      }
       if (exact) exact[i] = field_exact(F, x[0], x[1], x[2]) ? 1 : 0;
     }
   }
@@ -614,7 +707,7 @@ __global__ void __launch_bounds__(TC_ROWS) eval_tc_kernel(FieldK F, size_t n, co
 // relative force error of each coarse voxel (atomicMax on the float bits:
 // errors are non-negative).
 __global__ void validate_kernel(FieldK F, size_t n, const float4 *__restrict__ pos, const float *__restrict__ lab,
-                                int nf, float f0, float evox_inv, int ev, float *err_f, float *err_u,
+                                int nf, TrainGeo G, float evox_inv, int ev, float *err_f, float *err_u,
                                 unsigned int *vox_err) {
   const size_t w = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
@@ -623,14 +716,20 @@ __global__ void validate_kernel(FieldK F, size_t n, const float4 *__restrict__ p
     const float4 p = pos[i];
     const float x[3] = {p.x, p.y, p.z};
     float emax = 0.f, eu = 0.f;
-    for (int fld = 0; fld < nf; fld++) {
-      float uu, ff[3];
-      field_site_warp(F, x, fld, uu, ff);
-      const float *lb = lab + (i * nf + fld) * 4;
-      const float dx = ff[0] - lb[1], dy = ff[1] - lb[2], dz = ff[2] - lb[3];
-      const float fn = sqrtf(lb[1] * lb[1] + lb[2] * lb[2] + lb[3] * lb[3]);
-      emax = fmaxf(emax, sqrtf(dx * dx + dy * dy + dz * dz) / (fn + f0));
-      eu = fmaxf(eu, fabsf(uu - lb[0]));
+    for (int f0i = 0; f0i < nf; f0i += FL_SITE_FIELDS) {
+      int fl[FL_SITE_FIELDS];
+      const int nfo = min(FL_SITE_FIELDS, nf - f0i);
+      for (int k = 0; k < FL_SITE_FIELDS; k++) fl[k] = min(f0i + k, nf - 1);
+      float uu[FL_SITE_FIELDS], ff[FL_SITE_FIELDS][3];
+      field_site_warp(F, x, nfo, fl, uu, ff);
+      for (int k = 0; k < nfo; k++) {
+        const int fld = fl[k];
+        const float *lb = lab + (i * nf + fld) * 4;
+        const float dx = ff[k][0] - lb[1], dy = ff[k][1] - lb[2], dz = ff[k][2] - lb[3];
+        const float fn = sqrtf(lb[1] * lb[1] + lb[2] * lb[2] + lb[3] * lb[3]);
+        emax = fmaxf(emax, sqrtf(dx * dx + dy * dy + dz * dz) / (fn + G.f0[fld]));
+        eu = fmaxf(eu, fabsf(uu[k] - lb[0]) / fmaxf(G.s[fld], 1e-30f));
+      }
     }
     if (lane == 0) {
       err_f[i] = emax;
@@ -690,22 +789,53 @@ void free_state(FieldState *fs) {
   dfree(fs->bidx);
 }
 
-// Field of each gas site and the site that represents each field in the labels.
-void site_fields(int gas, int &nf, int sf[3], int rep[FL_NF]) {
-  if (gas == CCS_GAS_N2) {  // N, N, central charge
-    nf = 2; sf[0] = 0; sf[1] = 0; sf[2] = 1; rep[0] = 0; rep[1] = 2;
-  } else if (gas == CCS_GAS_CO2) {  // O, C, O
-    nf = 2; sf[0] = 0; sf[1] = 1; sf[2] = 0; rep[0] = 0; rep[1] = 1;
-  } else {
-    nf = 1; sf[0] = sf[1] = sf[2] = 0; rep[0] = 0; rep[1] = 0;
+// The geometry and per-field scales and floors the training kernel reads.
+void refresh_geo(FieldState *fs) {
+  for (int f = 0; f < FL_NF; f++) {
+    fs->geo.s[f] = (float)fs->s[f];
+    fs->geo.u0[f] = (float)(fs->p.u0 * fs->s[f]);
+    fs->geo.f0[f] = (float)(fs->p.f0 * fs->gs[f]);
   }
+}
+
+// The fields of a context: the far potential of each gas site type (with
+// its LJ parameter set and charge), then, with the induced dipole, the three
+// far-field components; the field of each site and the dipole's site.
+void field_layout(const ccs_ctx *c, FieldState *fs) {
+  FieldKind &k = fs->kinds;
+  std::memset(&k, 0, sizeof k);
+  const int gas = c->p.gas;
+  const bool coul = c->coul_on != 0;
+  int nf = 0;
+  if (gas == CCS_GAS_N2) {  // N, N, central charge (GasBuffer.cpp:79-115)
+    k.lj[0] = 1; k.q[0] = coul ? -0.4825 : 0.0;
+    k.lj[1] = 0; k.q[1] = coul ? 0.965 : 0.0;
+    nf = 2;
+    fs->site_field[0] = fs->site_field[1] = 0; fs->site_field[2] = 1;
+    fs->dip_site = c->dip_on ? 2 : -1;
+  } else if (gas == CCS_GAS_CO2) {  // O, C, O (GasBuffer.cpp:116-165)
+    k.lj[0] = 1; k.q[0] = coul ? -0.3256 : 0.0;
+    k.lj[1] = 2; k.q[1] = coul ? 0.6512 : 0.0;
+    nf = 2;
+    fs->site_field[0] = fs->site_field[2] = 0; fs->site_field[1] = 1;
+    fs->dip_site = c->dip_on ? 1 : -1;
+  } else {  // atoms: LJ only (neutral probe)
+    k.lj[0] = 1; k.q[0] = 0.0;
+    nf = 1;
+    fs->site_field[0] = fs->site_field[1] = fs->site_field[2] = 0;
+    fs->dip_site = c->dip_on ? 0 : -1;
+  }
+  fs->efield = nf;
+  if (fs->dip_site >= 0)
+    for (int a = 0; a < 3; a++) { k.kind[nf] = 1; k.comp[nf] = a; nf++; }
+  fs->nf = nf;
 }
 
 // Geometry (domain cube, grids, bitmap dimensions), parameter memory and
 // random initial parameters.
 int setup_geometry(ccs_ctx *c, FieldState *fs, const ccs_field_params &p) {
   fs->p = p;
-  site_fields(c->p.gas, fs->nf, fs->site_field, fs->rep_site);
+  field_layout(c, fs);
   // the region a site can reach while the probe is within the force reach of
   // the target's bounding box, plus a margin
   const double margin = c->reach + 2.5 + 1.0;
@@ -744,6 +874,10 @@ int setup_geometry(ccs_ctx *c, FieldState *fs, const ccs_field_params &p) {
   K.vox_inv = (float)(1.0 / p.voxel);
   K.nf = fs->nf;
   for (int s = 0; s < 3; s++) K.site_field[s] = fs->site_field[s];
+  K.dip_site = fs->dip_site;
+  K.efield = fs->efield;
+  K.r_in = (float)p.r_in;
+  K.r_out = (float)p.r_out;
   fs->nwords = ((size_t)nv * nv * nv + 31) / 32;
   const size_t nt = (size_t)FL_LEVELS * fs->rows;
   int rc;
@@ -791,8 +925,8 @@ int setup_geometry(ccs_ctx *c, FieldState *fs, const ccs_field_params &p) {
   bitmap_atoms_kernel<<<(c->natoms + 127) / 128, 128, 0, c->stream>>>(c->d_xyzq32, c->natoms, K, (float)p.voxel, R,
                                                                      fs->bits);
   CK(cudaGetLastError());
-  fs->s = 1.0;
-  K.s = 1.f;
+  for (int f = 0; f < FL_NF; f++) fs->s[f] = fs->gs[f] = 1.0;
+  refresh_geo(fs);
   return CCS_OK;
 }
 
@@ -800,9 +934,11 @@ int pack_inference(ccs_ctx *c, FieldState *fs) {
   const size_t nt = (size_t)FL_LEVELS * fs->rows;
   table_to_bf16_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, c->stream>>>(fs->table, nt, fs->table_bf16);
   CK(cudaGetLastError());
-  pack_mlp_kernel<<<1, 256, 0, c->stream>>>(fs->mlp, fs->nf, fs->mlp_inf, reinterpret_cast<uint16_t *>(fs->umma));
+  FieldScales sc;
+  for (int f = 0; f < FL_NF; f++) sc.s[f] = (float)fs->s[f];
+  pack_mlp_kernel<<<1, 256, 0, c->stream>>>(fs->mlp, fs->nf, sc, fs->mlp_inf, reinterpret_cast<uint16_t *>(fs->umma));
   CK(cudaGetLastError());
-  fs->k.s = (float)fs->s;
+  refresh_geo(fs);
   return CCS_OK;
 }
 
@@ -859,23 +995,14 @@ int draw_samples(ccs_ctx *c, FieldState *fs, size_t n, uint64_t seed, float4 *&p
   CK(cudaStreamSynchronize(s));
   double t1 = now_ms();
   if (ms_sample) *ms_sample += t1 - t0;
-  // labels: each field's representative site at every sample (the engine's exact FP32 evaluator)
-  double *dp = nullptr, *df = nullptr, *dU = nullptr;
-  if ((rc = dalloc(c, dp, n * 3 * sizeof(double))) || (rc = dalloc(c, df, n * 3 * sizeof(double))) ||
-      (rc = dalloc(c, dU, n * sizeof(double))) || (rc = dalloc(c, lab, n * fs->nf * 4 * sizeof(float)))) {
-    dfree(dp); dfree(df); dfree(dU);
-    return rc;
-  }
-  pos_to_double_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(pos, n, dp);
+  // labels: the far parts of every field at every sample
+  if ((rc = dalloc(c, lab, n * fs->nf * 4 * sizeof(float)))) return rc;
+  KParams kp = base_params(c);
+  kp.field = fs->k;
+  far_label_kernel<<<(unsigned)std::min<size_t>((n + 7) / 8, (size_t)c->sm_count * 64), 256, 0, s>>>(
+      kp, fs->kinds, fs->nf, n, pos, lab);
   CK(cudaGetLastError());
-  for (int f = 0; f < fs->nf; f++) {
-    rc = eval_site_forces_device(c, n, fs->rep_site[f], dp, df, dU, s);
-    if (rc) break;
-    pack_labels_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(df, dU, n, f, fs->nf, lab);
-    CK(cudaGetLastError());
-  }
   CK(cudaStreamSynchronize(s));
-  dfree(dp); dfree(df); dfree(dU);
   if (ms_label) *ms_label += now_ms() - t1;
   return rc;
 }
@@ -900,25 +1027,30 @@ constexpr size_t TRAIN_SMEM = (size_t)(2 * FL_H * FL_E + 2 * FL_H * FL_H + 2 * F
 
 // Loss gradients of one batch (indices already in fs->bidx) into fs->mgrad
 // and fs->tgrad; the batch's mean loss into *loss_dev.
+template <int NF>
+void launch_train(ccs_ctx *c, FieldState *fs, const float4 *pos, const float *lab, int B, int grid, float invB,
+                  cudaStream_t s) {
+  train_kernel<NF><<<grid, 256, TRAIN_SMEM, s>>>(fs->table, fs->mlp, fs->geo, pos, lab, fs->bidx, B,
+                                                 (float)fs->p.lam_u, invB, fs->L1, fs->R1, fs->L2, fs->R2, fs->V3,
+                                                 fs->lossbuf, fs->tgrad);
+  const int nparts = (B + WG_CH - 1) / WG_CH;
+  wgrad_kernel<NF><<<nparts, 256, 0, s>>>(fs->L1, fs->R1, fs->L2, fs->R2, fs->V3, B, fs->part);
+}
+
+// Loss gradients of one batch (indices already in fs->bidx) into fs->mgrad
+// and fs->tgrad; the batch's mean loss into *loss_dev.
 int grad_step(ccs_ctx *c, FieldState *fs, const float4 *pos, const float *lab, int B, float *loss_dev) {
   cudaStream_t s = c->stream;
-  const ccs_field_params &p = fs->p;
   const int grid = std::max(1, std::min(c->sm_count * 8, (B + 7) / 8));
   const float invB = 1.0f / (float)B;
-  if (fs->nf == 2) {
-    train_kernel<2><<<grid, 256, TRAIN_SMEM, s>>>(fs->table, fs->mlp, fs->geo, (float)fs->s, pos, lab, fs->bidx, B,
-                                                  (float)p.lam_u, (float)p.u0, (float)p.f0, invB, fs->L1, fs->R1,
-                                                  fs->L2, fs->R2, fs->V3, fs->lossbuf, fs->tgrad);
-  } else {
-    train_kernel<1><<<grid, 256, TRAIN_SMEM, s>>>(fs->table, fs->mlp, fs->geo, (float)fs->s, pos, lab, fs->bidx, B,
-                                                  (float)p.lam_u, (float)p.u0, (float)p.f0, invB, fs->L1, fs->R1,
-                                                  fs->L2, fs->R2, fs->V3, fs->lossbuf, fs->tgrad);
+  switch (fs->nf) {
+    case 1: launch_train<1>(c, fs, pos, lab, B, grid, invB, s); break;
+    case 2: launch_train<2>(c, fs, pos, lab, B, grid, invB, s); break;
+    case 4: launch_train<4>(c, fs, pos, lab, B, grid, invB, s); break;
+    default: launch_train<5>(c, fs, pos, lab, B, grid, invB, s); break;
   }
   CK(cudaGetLastError());
   const int nparts = (B + WG_CH - 1) / WG_CH;
-  if (fs->nf == 2) wgrad_kernel<2><<<nparts, 256, 0, s>>>(fs->L1, fs->R1, fs->L2, fs->R2, fs->V3, B, fs->part);
-  else wgrad_kernel<1><<<nparts, 256, 0, s>>>(fs->L1, fs->R1, fs->L2, fs->R2, fs->V3, B, fs->part);
-  CK(cudaGetLastError());
   sum_partials_kernel<<<(NM + 255) / 256, 256, 0, s>>>(fs->part, nparts, fs->mgrad);
   CK(cudaGetLastError());
   if (loss_dev) {
@@ -934,6 +1066,8 @@ int attr_once(ccs_ctx *c) {
   if (done[c->device]) return CCS_OK;
   CK(cudaFuncSetAttribute(train_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM));
   CK(cudaFuncSetAttribute(train_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM));
+  CK(cudaFuncSetAttribute(train_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM));
+  CK(cudaFuncSetAttribute(train_kernel<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM));
   CK(cudaFuncSetAttribute(eval_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
   done[c->device] = true;
   return CCS_OK;
@@ -958,6 +1092,7 @@ int check_params(ccs_ctx *c, const ccs_field_params *p) {
   if (p->samples < 1024 || p->batch < 32 || p->iterations < 0 || p->validation < 0)
     return fail(c, CCS_ERR_INVALID, "samples >= 1024, batch >= 32, iterations and validation >= 0");
   if ((size_t)p->batch > (size_t)p->samples) return fail(c, CCS_ERR_INVALID, "batch exceeds samples");
+  if (!(p->r_in > 0) || !(p->r_out > p->r_in)) return fail(c, CCS_ERR_INVALID, "need 0 < r_in < r_out");
   return CCS_OK;
 }
 
@@ -973,7 +1108,10 @@ void fill_report(const FieldState *fs, ccs_field_report *r) {
   }
   r->nfields = fs->nf;
   r->log2_table = fs->p.log2_table;
-  r->output_scale = fs->s;
+  for (int f = 0; f < FL_NF; f++) {
+    r->output_scale[f] = fs->s[f];
+    r->gradient_scale[f] = fs->gs[f];
+  }
 }
 
 }  // namespace
@@ -1018,6 +1156,8 @@ void ccs_field_params_default(ccs_field_params *p) {
   p->u0 = 0.05;
   p->f0 = 0.05;
   p->seed = 2104;
+  p->r_in = 6.0;
+  p->r_out = 8.0;
 }
 
 int ccs_field_setup(ccs_ctx *c, const ccs_field_params *p, ccs_field_report *report) {
@@ -1058,13 +1198,23 @@ int ccs_field_train(ccs_ctx *c, const ccs_field_params *p, ccs_field_report *rep
   if ((rc = draw_samples(c, fs, fs->nsamples, p->seed, fs->spos, fs->slab, &rep.sample_ms, &rep.label_ms)))
     return bail(rc);
   rep.samples = (int64_t)fs->nsamples;
-  {  // output scale: RMS of the potential labels
+  {  // per field: output scale = RMS of its values, gradient scale = RMS of |gradient|
     std::vector<float> lab(fs->nsamples * fs->nf * 4);
     if (cudaMemcpy(lab.data(), fs->slab, lab.size() * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
       return bail(fail(c, CCS_ERR_CUDA, "label copy"));
-    double ss = 0.0;
-    for (size_t i = 0; i < fs->nsamples * fs->nf; i++) ss += (double)lab[4 * i] * lab[4 * i];
-    fs->s = std::max(1e-3, std::sqrt(ss / (double)(fs->nsamples * fs->nf)));
+    for (int f = 0; f < fs->nf; f++) {
+      double su = 0.0, sg = 0.0;
+      for (size_t i = 0; i < fs->nsamples; i++) {
+        const float *l = &lab[(i * fs->nf + f) * 4];
+        su += (double)l[0] * l[0];
+        sg += (double)l[1] * l[1] + (double)l[2] * l[2] + (double)l[3] * l[3];
+      }
+      fs->s[f] = std::max(1e-12, std::sqrt(su / (double)fs->nsamples));
+      fs->gs[f] = std::max(1e-12, std::sqrt(sg / (double)fs->nsamples));
+      rep.output_scale[f] = fs->s[f];
+      rep.gradient_scale[f] = fs->gs[f];
+    }
+    refresh_geo(fs);
   }
   // ---- training
   const int B = p->batch;
@@ -1120,7 +1270,7 @@ int ccs_field_train(ccs_ctx *c, const ccs_field_params *p, ccs_field_report *rep
     cudaMemsetAsync(verr, 0, (size_t)ev * ev * ev * sizeof(unsigned int), s);
     cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), s);
     FieldK K = fs->k;
-    validate_kernel<<<c->sm_count * 8, 256, 0, s>>>(K, nv, vpos, vlab, fs->nf, (float)p->f0,
+    validate_kernel<<<c->sm_count * 8, 256, 0, s>>>(K, nv, vpos, vlab, fs->nf, fs->geo,
                                                      (float)(1.0 / p->err_voxel), ev, ef, eu, verr);
     flag_err_voxels_kernel<<<(unsigned)(((size_t)ev * ev * ev + 255) / 256), 256, 0, s>>>(
         K, verr, ev, ratio, (float)p->err_threshold, fs->bits, cnt);
@@ -1140,7 +1290,7 @@ int ccs_field_train(ccs_ctx *c, const ccs_field_params *p, ccs_field_report *rep
     std::nth_element(sorted.begin(), sorted.begin() + q, sorted.end());
     rep.val_force_rel_rms = std::sqrt(sf / (double)nv);
     rep.val_force_rel_p99 = sorted[q];
-    rep.val_u_abs_rms = std::sqrt(su / (double)nv);
+    rep.val_u_rel_rms = std::sqrt(su / (double)nv);
     rep.err_voxels = (int64_t)hc[0];
     rep.exact_fraction = (double)hc[1] / ((double)fs->k.vx * fs->k.vy * fs->k.vz);
     rep.validate_ms = now_ms() - tv0;
@@ -1167,8 +1317,8 @@ int ccs_field_enable(ccs_ctx *c, int on) {
   return CCS_OK;
 }
 
-int ccs_field_eval(ccs_ctx *c, size_t n, int site, const double *pos, int path, double *u, double *f,
-                   int8_t *exact) {
+int ccs_field_eval(ccs_ctx *c, size_t n, int site, const double *pos, int path, double *u, double *g,
+                   int8_t *exact, int32_t *nfields) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!(c->field && c->field->ready)) return fail(c, CCS_ERR_INVALID, "no learned field");
@@ -1176,36 +1326,38 @@ int ccs_field_eval(ccs_ctx *c, size_t n, int site, const double *pos, int path, 
   const int ns = is_molecule(c->p.gas) ? 3 : 1;
   if (site < 0 || site >= ns) return fail(c, CCS_ERR_INVALID, "site out of range");
   if (path != 0 && path != 1) return fail(c, CCS_ERR_INVALID, "path must be 0 (tensor cores) or 1 (warp)");
+  if (nfields) *nfields = site == fs->dip_site ? 4 : 1;
   if (n == 0) return CCS_OK;
-  if (!pos || !u || !f) return fail(c, CCS_ERR_INVALID, "pos, u and f are required");
+  if (!pos || !u || !g) return fail(c, CCS_ERR_INVALID, "pos, u and g are required");
   std::vector<float4> hp(n);
   for (size_t i = 0; i < n; i++) hp[i] = make_float4((float)pos[3 * i], (float)pos[3 * i + 1], (float)pos[3 * i + 2], 0.f);
   float4 *dp = nullptr;
-  double *du = nullptr, *df = nullptr;
+  double *du = nullptr, *dg = nullptr;
   int8_t *dx = nullptr;
   int *derr = nullptr;
-  auto cleanup = [&]() { dfree(dp); dfree(du); dfree(df); dfree(dx); dfree(derr); };
-  if ((rc = dalloc(c, dp, n * sizeof(float4))) || (rc = dalloc(c, du, n * sizeof(double))) ||
-      (rc = dalloc(c, df, n * 3 * sizeof(double))) || (rc = dalloc(c, dx, n)) || (rc = dalloc(c, derr, sizeof(int)))) {
+  auto cleanup = [&]() { dfree(dp); dfree(du); dfree(dg); dfree(dx); dfree(derr); };
+  if ((rc = dalloc(c, dp, n * sizeof(float4))) || (rc = dalloc(c, du, n * 4 * sizeof(double))) ||
+      (rc = dalloc(c, dg, n * 12 * sizeof(double))) || (rc = dalloc(c, dx, n)) || (rc = dalloc(c, derr, sizeof(int)))) {
     cleanup();
     return rc;
   }
   int herr = 0;
   bool ok = cudaMemcpy(dp, hp.data(), n * sizeof(float4), cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemset(du, 0, n * 4 * sizeof(double)) == cudaSuccess &&
+            cudaMemset(dg, 0, n * 12 * sizeof(double)) == cudaSuccess &&
             cudaMemset(derr, 0, sizeof(int)) == cudaSuccess;
-  const int field = fs->site_field[site];
   if (ok) {
     if (path == 0) {
       const size_t tiles = (n + TC_ROWS - 1) / TC_ROWS;
       const unsigned grid = (unsigned)std::min<size_t>(tiles, (size_t)c->sm_count * 2);
-      eval_tc_kernel<<<grid, TC_ROWS, TC_SMEM_BYTES, c->stream>>>(fs->k, n, dp, field, du, df, dx, derr);
+      eval_tc_kernel<<<grid, TC_ROWS, TC_SMEM_BYTES, c->stream>>>(fs->k, n, dp, site, du, dg, dx, derr);
     } else {
       eval_warp_kernel<<<(unsigned)std::min<size_t>((n + 7) / 8, (size_t)c->sm_count * 16), 256, 0, c->stream>>>(
-          fs->k, n, dp, field, du, df, dx);
+          fs->k, n, dp, site, du, dg, dx);
     }
     ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(c->stream) == cudaSuccess &&
-         cudaMemcpy(u, du, n * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess &&
-         cudaMemcpy(f, df, n * 3 * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(u, du, n * 4 * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(g, dg, n * 12 * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess &&
          (!exact || cudaMemcpy(exact, dx, n, cudaMemcpyDeviceToHost) == cudaSuccess) &&
          cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess;
   }
@@ -1215,7 +1367,38 @@ int ccs_field_eval(ccs_ctx *c, size_t n, int site, const double *pos, int path, 
   return CCS_OK;
 }
 
-int ccs_field_get_weights(ccs_ctx *c, float *table, float *mlp, double *output_scale) {
+int ccs_field_labels(ccs_ctx *c, size_t n, const double *pos, double *labels) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->field) return fail(c, CCS_ERR_INVALID, "no learned field: call ccs_field_setup");
+  if (n == 0) return CCS_OK;
+  if (!pos || !labels) return fail(c, CCS_ERR_INVALID, "pos and labels are required");
+  FieldState *fs = c->field;
+  std::vector<float4> hp(n);
+  for (size_t i = 0; i < n; i++) hp[i] = make_float4((float)pos[3 * i], (float)pos[3 * i + 1], (float)pos[3 * i + 2], 0.f);
+  float4 *dp = nullptr;
+  float *dl = nullptr;
+  if ((rc = dalloc(c, dp, n * sizeof(float4))) || (rc = dalloc(c, dl, n * fs->nf * 4 * sizeof(float)))) {
+    dfree(dp); dfree(dl);
+    return rc;
+  }
+  KParams kp = base_params(c);
+  kp.field = fs->k;
+  std::vector<float> hl(n * fs->nf * 4);
+  bool ok = cudaMemcpy(dp, hp.data(), n * sizeof(float4), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (ok) {
+    far_label_kernel<<<(unsigned)std::min<size_t>((n + 7) / 8, (size_t)c->sm_count * 64), 256, 0, c->stream>>>(
+        kp, fs->kinds, fs->nf, n, dp, dl);
+    ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(c->stream) == cudaSuccess &&
+         cudaMemcpy(hl.data(), dl, hl.size() * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess;
+  }
+  dfree(dp); dfree(dl);
+  if (!ok) return fail(c, CCS_ERR_CUDA, "field labels: %s", cudaGetErrorString(cudaGetLastError()));
+  for (size_t i = 0; i < hl.size(); i++) labels[i] = hl[i];
+  return CCS_OK;
+}
+
+int ccs_field_get_weights(ccs_ctx *c, float *table, float *mlp, double *scales) {
   if (!c) return CCS_ERR_INVALID;
   if (!c->field) return fail(c, CCS_ERR_INVALID, "no learned field");
   FieldState *fs = c->field;
@@ -1231,15 +1414,18 @@ int ccs_field_get_weights(ccs_ctx *c, float *table, float *mlp, double *output_s
     std::memcpy(mlp + MO_W3, m.data() + MO_W3, fs->nf * FL_H * sizeof(float));
     std::memcpy(mlp + MO_W3 + fs->nf * FL_H, m.data() + MO_B3, fs->nf * sizeof(float));
   }
-  if (output_scale) *output_scale = fs->s;
+  if (scales)
+    for (int f = 0; f < fs->nf; f++) { scales[f] = fs->s[f]; scales[fs->nf + f] = fs->gs[f]; }
   return CCS_OK;
 }
 
-int ccs_field_set_weights(ccs_ctx *c, const float *table, const float *mlp, double output_scale) {
+int ccs_field_set_weights(ccs_ctx *c, const float *table, const float *mlp, const double *scales) {
   if (!c) return CCS_ERR_INVALID;
   if (!c->field) return fail(c, CCS_ERR_INVALID, "no learned field: call ccs_field_setup");
-  if (!(output_scale > 0)) return fail(c, CCS_ERR_INVALID, "output_scale must be positive");
   FieldState *fs = c->field;
+  if (scales)
+    for (int f = 0; f < 2 * fs->nf; f++)
+      if (!(scales[f] > 0)) return fail(c, CCS_ERR_INVALID, "scales must be positive");
   if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
   const size_t nt = (size_t)FL_LEVELS * fs->rows;
   if (table) CK(cudaMemcpy(fs->table, table, nt * sizeof(float2), cudaMemcpyHostToDevice));
@@ -1250,7 +1436,8 @@ int ccs_field_set_weights(ccs_ctx *c, const float *table, const float *mlp, doub
     std::memcpy(m.data() + MO_B3, mlp + MO_W3 + fs->nf * FL_H, fs->nf * sizeof(float));
     CK(cudaMemcpy(fs->mlp, m.data(), NM * sizeof(float), cudaMemcpyHostToDevice));
   }
-  fs->s = output_scale;
+  if (scales)
+    for (int f = 0; f < fs->nf; f++) { fs->s[f] = scales[f]; fs->gs[f] = scales[fs->nf + f]; }
   int rc = pack_inference(c, fs);
   if (rc) return rc;
   CK(cudaStreamSynchronize(c->stream));

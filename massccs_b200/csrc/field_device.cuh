@@ -4,13 +4,22 @@
 // (src/Force.cpp:34-1725); the field replaces those sums where it is
 // trusted, and the exact evaluation stays everywhere else.
 //
+// Range separation: every pair term (LJ, Coulomb, the dipole's field) is
+// split by a smooth switch S(r) (1 below r_in, 0 above r_out, quintic
+// smootherstep between) into a near part S * term, summed exactly over the
+// atoms within r_out of the site, and a far part (1 - S) * term, which is a
+// smooth function of the site position (no atom closer than r_in
+// contributes) and is what the network learns.
+//
 // Model (the checker is oracle/surrogate.py): a multiresolution hash-grid
 // encoding of the site position (16 levels x 2 features, smoothstep blending,
 // so the encoding has continuous first derivatives) feeds a ReLU MLP
-// 32 -> 64 -> 64 -> nf whose outputs are the potentials u_f of the gas's site
-// types (N2: the N atoms and the central charge; CO2: O and C; atoms: one).
-// A site's force is minus the gradient of its potential, back-propagated
-// through the MLP and the encoding, so the field is conservative.
+// 32 -> 64 -> 64 -> nf with per-field output scales.  Fields: the far
+// potential of each gas site type (N2: the N atoms and the central charge;
+// CO2: O and C; atoms: one) and, with the induced dipole, the three
+// components of the far electric field.  Each field's gradient is
+// back-propagated through the MLP and the encoding: the far forces are
+// conservative, and the far field's gradients give its Jacobian.
 //
 // Inference arithmetic (identical in both paths below, up to FP32 summation
 // order): table and the W1/W2 weights in bfloat16, the MMA inputs (encoded
@@ -37,7 +46,8 @@ constexpr int FL_LEVELS = 16;              // hash-grid levels
 constexpr int FL_FEAT = 2;                 // features per level
 constexpr int FL_E = FL_LEVELS * FL_FEAT;  // encoded features (32)
 constexpr int FL_H = 64;                   // hidden width
-constexpr int FL_NF = 2;                   // most output fields (site types)
+constexpr int FL_NF = 5;                   // most output fields (2 site types + 3 field components)
+constexpr int FL_SITE_FIELDS = 4;          // most fields evaluated at one site (the dipole site)
 
 // Offsets (floats) of the FP32 copies of the (bf16-rounded) MLP in FieldK::mlp.
 constexpr int FO_W1 = 0;                          // W1  [64][32]
@@ -48,7 +58,8 @@ constexpr int FO_B1 = FO_W2T + FL_H * FL_H;       // b1  [64]
 constexpr int FO_B2 = FO_B1 + FL_H;               // b2  [64]
 constexpr int FO_W3 = FO_B2 + FL_H;               // w3  [FL_NF][64] (FP32, not rounded)
 constexpr int FO_B3 = FO_W3 + FL_NF * FL_H;       // b3  [FL_NF]
-constexpr int FO_TOTAL = FO_B3 + FL_NF;
+constexpr int FO_S = FO_B3 + FL_NF;               // s   [FL_NF] output scales
+constexpr int FO_TOTAL = FO_S + FL_NF;
 
 // Byte offsets of the tcgen05 B-operand images in FieldK::umma (each in the
 // K-major no-swizzle core-matrix layout: element (row n, k) at
@@ -74,11 +85,31 @@ struct FieldK {
   int log2t;
   float vox_inv;               // 1 / voxel edge of the exact-evaluation bitmap
   int vx, vy, vz;              // bitmap dimensions (voxels from lo)
-  float s;                     // output scale (kcal/mol)
+  float r_in, r_out;           // range separation: the switch runs from r_in to r_out (A)
   int nf;                      // output fields
-  int site_field[3];           // field of each gas site
+  int site_field[3];           // far-potential field of each gas site
+  int dip_site;                // the induced dipole's site (-1: none)
+  int efield;                  // first of the three far-field components (E_x, E_y, E_z)
   int on;
 };
+
+// The fields evaluated at site s: its far potential, and at the dipole site
+// the three far-field components.  Returns their count.
+__device__ __forceinline__ int site_fields(const FieldK &F, int s, int (&fl)[FL_SITE_FIELDS]) {
+  fl[0] = F.site_field[s];
+  if (s != F.dip_site) return 1;
+  fl[1] = F.efield; fl[2] = F.efield + 1; fl[3] = F.efield + 2;
+  return 4;
+}
+
+// The switch of the range separation and its derivative d/dr.
+template <typename T> __device__ __forceinline__ void range_switch(T r, T r_in, T r_out, T &S, T &dS) {
+  const T w = r_out - r_in;
+  T x = (r - r_in) / w;
+  x = x < T(0) ? T(0) : (x > T(1) ? T(1) : x);
+  S = T(1) - x * x * x * (T(10) - T(15) * x + T(6) * x * x);
+  dS = T(-30) * x * x * (T(1) - x) * (T(1) - x) / w;
+}
 
 // ---- exact-evaluation test --------------------------------------------------
 // Positions outside the domain, within the fallback radius of an atom, or in
@@ -158,9 +189,11 @@ __device__ __forceinline__ void field_encode(const FieldK &F, const float (&x)[3
 
 // ---- warp path: one site evaluated by one warp ------------------------------
 // Lane l holds feature l (level l / 2) with its Jacobian row, and hidden units
-// 2l, 2l + 1.  Returns u and the force of field f at x in every lane.
-__device__ __forceinline__ void field_site_warp(const FieldK &F, const float (&x)[3], int f, float &u,
-                                                float (&force)[3]) {
+// 2l, 2l + 1.  For each of the nfo fields fl[k]: its value u[k] and minus its
+// gradient g[k] (for a potential: the force), in every lane.
+__device__ __forceinline__ void field_site_warp(const FieldK &F, const float (&x)[3], int nfo,
+                                                const int (&fl)[FL_SITE_FIELDS], float (&u)[FL_SITE_FIELDS],
+                                                float (&g)[FL_SITE_FIELDS][3]) {
   const int lane = threadIdx.x & 31;
   constexpr unsigned FULL = 0xffffffffu;
   // encoding: lane l takes level l >> 1, corners 4 (l & 1) .. + 3
@@ -213,36 +246,41 @@ __device__ __forceinline__ void field_site_warp(const FieldK &F, const float (&x
     z2a += w.x * aj; z2b += w.y * aj;
   }
   const bool m2a = z2a > 0.f, m2b = z2b > 0.f;
-  const float w3a = __ldg(&M[FO_W3 + f * FL_H + 2 * lane]), w3b = __ldg(&M[FO_W3 + f * FL_H + 2 * lane + 1]);
-  float up = (m2a ? z2a * w3a : 0.f) + (m2b ? z2b * w3b : 0.f);
+#pragma unroll 1
+  for (int k = 0; k < nfo; k++) {
+    const int f = fl[k];
+    const float sf = __ldg(&M[FO_S + f]);
+    const float w3a = __ldg(&M[FO_W3 + f * FL_H + 2 * lane]), w3b = __ldg(&M[FO_W3 + f * FL_H + 2 * lane + 1]);
+    float up = (m2a ? z2a * w3a : 0.f) + (m2b ? z2b * w3b : 0.f);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) up += __shfl_xor_sync(FULL, up, o);
-  u = F.s * (up + __ldg(&M[FO_B3 + f]));
-  // g2 = w3_f * m2 ; g1 = m1 * (W2^T g2) ; g0 = W1^T g1 ; F = -s J^T g0
-  const float g2a = bf16r(m2a ? w3a : 0.f), g2b = bf16r(m2b ? w3b : 0.f);
-  float g1a = 0.f, g1b = 0.f;
+    for (int o = 16; o > 0; o >>= 1) up += __shfl_xor_sync(FULL, up, o);
+    u[k] = sf * (up + __ldg(&M[FO_B3 + f]));
+    // g2 = w3_f * m2 ; g1 = m1 * (W2^T g2) ; g0 = W1^T g1 ; -grad = -s J^T g0
+    const float g2a = bf16r(m2a ? w3a : 0.f), g2b = bf16r(m2b ? w3b : 0.f);
+    float g1a = 0.f, g1b = 0.f;
 #pragma unroll 8
-  for (int o = 0; o < FL_H; o++) {
-    const float go = __shfl_sync(FULL, (o & 1) ? g2b : g2a, o >> 1);
-    const float2 w = __ldg(reinterpret_cast<const float2 *>(&M[FO_W2 + o * FL_H + 2 * lane]));
-    g1a += w.x * go; g1b += w.y * go;
-  }
-  g1a = bf16r(m1a ? g1a : 0.f);
-  g1b = bf16r(m1b ? g1b : 0.f);
-  float g0 = 0.f;  // feature `lane`
+    for (int o = 0; o < FL_H; o++) {
+      const float go = __shfl_sync(FULL, (o & 1) ? g2b : g2a, o >> 1);
+      const float2 w = __ldg(reinterpret_cast<const float2 *>(&M[FO_W2 + o * FL_H + 2 * lane]));
+      g1a += w.x * go; g1b += w.y * go;
+    }
+    g1a = bf16r(m1a ? g1a : 0.f);
+    g1b = bf16r(m1b ? g1b : 0.f);
+    float g0 = 0.f;  // feature `lane`
 #pragma unroll 8
-  for (int i = 0; i < FL_H; i++) {
-    const float gi = __shfl_sync(FULL, (i & 1) ? g1b : g1a, i >> 1);
-    g0 += __ldg(&M[FO_W1 + i * FL_E + lane]) * gi;
-  }
-  float fx = g0 * Jk[0], fy = g0 * Jk[1], fz = g0 * Jk[2];
+    for (int i = 0; i < FL_H; i++) {
+      const float gi = __shfl_sync(FULL, (i & 1) ? g1b : g1a, i >> 1);
+      g0 += __ldg(&M[FO_W1 + i * FL_E + lane]) * gi;
+    }
+    float fx = g0 * Jk[0], fy = g0 * Jk[1], fz = g0 * Jk[2];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    fx += __shfl_xor_sync(FULL, fx, o);
-    fy += __shfl_xor_sync(FULL, fy, o);
-    fz += __shfl_xor_sync(FULL, fz, o);
+    for (int o = 16; o > 0; o >>= 1) {
+      fx += __shfl_xor_sync(FULL, fx, o);
+      fy += __shfl_xor_sync(FULL, fy, o);
+      fz += __shfl_xor_sync(FULL, fz, o);
+    }
+    g[k][0] = -sf * fx; g[k][1] = -sf * fy; g[k][2] = -sf * fz;
   }
-  force[0] = -F.s * fx; force[1] = -F.s * fy; force[2] = -F.s * fz;
 }
 
 // ---- tensor-core path (tcgen05) ---------------------------------------------
@@ -405,13 +443,16 @@ __device__ __forceinline__ void tc_store_row(unsigned char *sm, int off, int row
   }
 }
 
-// The whole MLP of one site for the CTA's 128 rows (row = threadIdx.x).
-// use: this row holds a site to evaluate (others contribute zero rows);
-// e/J: its encoding and Jacobian; f: its output field.  Out: u and force.
-// Returns false if an MMA stage timed out (the caller stops the kernel).
+// The whole MLP of one site position for the CTA's 128 rows (row =
+// threadIdx.x), for the nfo fields fl[] (the same in every row): forward
+// once, then one backward chain per field.  use: this row holds a position
+// to evaluate (others contribute zero rows); e/J: its encoding and Jacobian.
+// Out: u[k] and minus the gradient g[k] of field fl[k].  Returns false if an
+// MMA stage timed out (the caller stops the kernel).
 __device__ __forceinline__ bool tc_site(const FieldK &F, unsigned char *sm, uint32_t tmem, uint32_t &phase,
-                                        bool use, const float (&e)[FL_E], const float (&J)[FL_E][3], int f,
-                                        float &u, float (&force)[3]) {
+                                        bool use, const float (&e)[FL_E], const float (&J)[FL_E][3], int nfo,
+                                        const int (&fl)[FL_SITE_FIELDS], float (&u)[FL_SITE_FIELDS],
+                                        float (&g)[FL_SITE_FIELDS][3]) {
   const int row = threadIdx.x;
   const uint32_t trow = tmem + ((uint32_t)(threadIdx.x & ~31) << 16);  // this warp's TMEM lanes
   const float *M = F.mlp;
@@ -442,10 +483,10 @@ __device__ __forceinline__ bool tc_site(const FieldK &F, unsigned char *sm, uint
     tc_store_row<FL_H>(sm, TC_SH, row, pk);
   }
   if (!tc_stage(sm, tmem, TC_SH, TC_SB + FU_W2, FL_H, FL_H, phase)) return false;
-  // epilogue 2: z2 + b2, relu, u = s (w3_f . a2 + b3_f); G2 = w3_f * m2 (bf16)
+  // epilogue 2: z2 + b2, mask m2, u_f = s_f (w3_f . relu(z2) + b3_f) for every field
+  uint32_t m2 = 0u, m2b = 0u;
   {
-    uint32_t pk[FL_H / 2];
-    float acc = 0.f;
+    float acc[FL_SITE_FIELDS] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       float v[16];
@@ -454,45 +495,64 @@ __device__ __forceinline__ bool tc_site(const FieldK &F, unsigned char *sm, uint
       for (int i = 0; i < 16; i += 2) {
         const int n = 16 * q + i;
         const float za = v[i] + __ldg(&M[FO_B2 + n]), zb = v[i + 1] + __ldg(&M[FO_B2 + n + 1]);
-        const float wa = __ldg(&M[FO_W3 + f * FL_H + n]), wb = __ldg(&M[FO_W3 + f * FL_H + n + 1]);
-        acc += (za > 0.f ? za * wa : 0.f) + (zb > 0.f ? zb * wb : 0.f);
-        pk[n / 2] = pack_bf16x2(za > 0.f ? wa : 0.f, zb > 0.f ? wb : 0.f);
+        const uint32_t bits = (za > 0.f ? 1u : 0u) | (zb > 0.f ? 2u : 0u);
+        if (n < 32) m2 |= bits << n; else m2b |= bits << (n - 32);
+        const float aa = fmaxf(za, 0.f), ab = fmaxf(zb, 0.f);
+#pragma unroll
+        for (int k = 0; k < FL_SITE_FIELDS; k++)
+          if (k < nfo) acc[k] += aa * __ldg(&M[FO_W3 + fl[k] * FL_H + n]) + ab * __ldg(&M[FO_W3 + fl[k] * FL_H + n + 1]);
       }
     }
-    u = F.s * (acc + __ldg(&M[FO_B3 + f]));
-    tc_store_row<FL_H>(sm, TC_SH, row, pk);
-  }
-  if (!tc_stage(sm, tmem, TC_SH, TC_SB + FU_W2T, FL_H, FL_H, phase)) return false;
-  // epilogue 3: G1 = m1 * (W2^T G2) (bf16)
-  {
-    uint32_t pk[FL_H / 2];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
+    for (int k = 0; k < FL_SITE_FIELDS; k++)
+      if (k < nfo) u[k] = __ldg(&M[FO_S + fl[k]]) * (acc[k] + __ldg(&M[FO_B3 + fl[k]]));
+  }
+#pragma unroll 1
+  for (int k = 0; k < nfo; k++) {
+    const int f = fl[k];
+    {  // G2 = w3_f * m2 (bf16)
+      uint32_t pk[FL_H / 2];
+#pragma unroll
+      for (int n = 0; n < FL_H; n += 2) {
+        const uint32_t mm = n < 32 ? (m2 >> n) : (m2b >> (n - 32));
+        pk[n / 2] = pack_bf16x2((mm & 1u) ? __ldg(&M[FO_W3 + f * FL_H + n]) : 0.f,
+                                (mm & 2u) ? __ldg(&M[FO_W3 + f * FL_H + n + 1]) : 0.f);
+      }
+      tc_store_row<FL_H>(sm, TC_SH, row, pk);
+    }
+    if (!tc_stage(sm, tmem, TC_SH, TC_SB + FU_W2T, FL_H, FL_H, phase)) return false;
+    // epilogue 3: G1 = m1 * (W2^T G2) (bf16)
+    {
+      uint32_t pk[FL_H / 2];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        float v[16];
+        tc_ld16(trow + 16 * q, v);
+#pragma unroll
+        for (int i = 0; i < 16; i += 2) {
+          const int n = 16 * q + i;
+          const uint32_t mm = n < 32 ? (m1 >> n) : (m1b >> (n - 32));
+          pk[n / 2] = pack_bf16x2((mm & 1u) ? v[i] : 0.f, (mm & 2u) ? v[i + 1] : 0.f);
+        }
+      }
+      tc_store_row<FL_H>(sm, TC_SH, row, pk);
+    }
+    if (!tc_stage(sm, tmem, TC_SH, TC_SB + FU_W1T, FL_H, FL_E, phase)) return false;
+    // epilogue 4: g0 = W1^T G1 (32), -grad = -s_f J^T g0
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
       float v[16];
       tc_ld16(trow + 16 * q, v);
 #pragma unroll
-      for (int i = 0; i < 16; i += 2) {
-        const int n = 16 * q + i;
-        const uint32_t mm = n < 32 ? (m1 >> n) : (m1b >> (n - 32));
-        pk[n / 2] = pack_bf16x2((mm & 1u) ? v[i] : 0.f, (mm & 2u) ? v[i + 1] : 0.f);
+      for (int i = 0; i < 16; i++) {
+        const int kk = 16 * q + i;
+        fx += v[i] * J[kk][0]; fy += v[i] * J[kk][1]; fz += v[i] * J[kk][2];
       }
     }
-    tc_store_row<FL_H>(sm, TC_SH, row, pk);
+    const float sf = __ldg(&M[FO_S + f]);
+    g[k][0] = -sf * fx; g[k][1] = -sf * fy; g[k][2] = -sf * fz;
   }
-  if (!tc_stage(sm, tmem, TC_SH, TC_SB + FU_W1T, FL_H, FL_E, phase)) return false;
-  // epilogue 4: g0 = W1^T G1 (32), F = -s J^T g0
-  float fx = 0.f, fy = 0.f, fz = 0.f;
-#pragma unroll
-  for (int q = 0; q < 2; q++) {
-    float v[16];
-    tc_ld16(trow + 16 * q, v);
-#pragma unroll
-    for (int i = 0; i < 16; i++) {
-      const int k = 16 * q + i;
-      fx += v[i] * J[k][0]; fy += v[i] * J[k][1]; fz += v[i] * J[k][2];
-    }
-  }
-  force[0] = -F.s * fx; force[1] = -F.s * fy; force[2] = -F.s * fz;
   return true;
 }
 

@@ -78,7 +78,7 @@ class CcsFieldParams(ctypes.Structure):
         ("fallback_radius", ctypes.c_double), ("voxel", ctypes.c_double), ("err_voxel", ctypes.c_double),
         ("err_threshold", ctypes.c_double), ("near_fraction", ctypes.c_double), ("near_shell", ctypes.c_double),
         ("lr", ctypes.c_double), ("lam_u", ctypes.c_double), ("u0", ctypes.c_double), ("f0", ctypes.c_double),
-        ("seed", ctypes.c_uint64),
+        ("seed", ctypes.c_uint64), ("r_in", ctypes.c_double), ("r_out", ctypes.c_double),
     ]
 
 
@@ -87,17 +87,20 @@ class CcsFieldReport(ctypes.Structure):
         ("domain_lo", ctypes.c_double * 3), ("domain_side", ctypes.c_double),
         ("levels", ctypes.c_int32), ("dense_levels", ctypes.c_int32), ("nfields", ctypes.c_int32),
         ("log2_table", ctypes.c_int32), ("res", ctypes.c_int32 * 16),
-        ("samples", ctypes.c_int64), ("output_scale", ctypes.c_double),
+        ("samples", ctypes.c_int64), ("output_scale", ctypes.c_double * 5),
+        ("gradient_scale", ctypes.c_double * 5),
         ("sample_ms", ctypes.c_double), ("label_ms", ctypes.c_double), ("train_ms", ctypes.c_double),
         ("validate_ms", ctypes.c_double), ("first_loss", ctypes.c_double), ("final_loss", ctypes.c_double),
         ("val_force_rel_rms", ctypes.c_double), ("val_force_rel_p99", ctypes.c_double),
-        ("val_u_abs_rms", ctypes.c_double), ("exact_fraction", ctypes.c_double), ("err_voxels", ctypes.c_int64),
+        ("val_u_rel_rms", ctypes.c_double), ("exact_fraction", ctypes.c_double), ("err_voxels", ctypes.c_int64),
     ]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
         d["domain_lo"] = list(self.domain_lo)
         d["res"] = list(self.res)
+        d["output_scale"] = list(self.output_scale)[:self.nfields]
+        d["gradient_scale"] = list(self.gradient_scale)[:self.nfields]
         return d
 
 
@@ -108,7 +111,7 @@ EXPORTS = ["ccs_version", "ccs_create", "ccs_destroy", "ccs_params_default", "cc
            "ccs_measure_fp32_peak", "ccs_run_device_noalloc", "ccs_run_batch",
            "ccs_field_params_default", "ccs_field_train", "ccs_field_enable", "ccs_field_eval",
            "ccs_field_setup", "ccs_field_get_weights", "ccs_field_set_weights", "ccs_field_loss_grad",
-           "ccs_equipotential_points"]
+           "ccs_equipotential_points", "ccs_field_labels"]
 
 _LIB = None
 
@@ -150,10 +153,11 @@ def load_library(path=LIB_PATH):
     L.ccs_field_train.argtypes = [vp, ctypes.POINTER(CcsFieldParams), ctypes.POINTER(CcsFieldReport)]
     L.ccs_field_setup.argtypes = [vp, ctypes.POINTER(CcsFieldParams), ctypes.POINTER(CcsFieldReport)]
     L.ccs_field_enable.argtypes = [vp, i32]
-    L.ccs_field_eval.argtypes = [vp, sz, i32, vp, i32, vp, vp, vp]
-    L.ccs_field_get_weights.argtypes = [vp, vp, vp, ctypes.POINTER(ctypes.c_double)]
-    L.ccs_field_set_weights.argtypes = [vp, vp, vp, ctypes.c_double]
+    L.ccs_field_eval.argtypes = [vp, sz, i32, vp, i32, vp, vp, vp, ctypes.POINTER(ctypes.c_int32)]
+    L.ccs_field_get_weights.argtypes = [vp, vp, vp, vp]
+    L.ccs_field_set_weights.argtypes = [vp, vp, vp, vp]
     L.ccs_field_loss_grad.argtypes = [vp, sz, vp, vp, ctypes.POINTER(ctypes.c_double), vp, vp]
+    L.ccs_field_labels.argtypes = [vp, sz, vp, vp]
     if path == LIB_PATH:
         _LIB = L
     return L
@@ -302,14 +306,17 @@ class Engine:
         self._check(self._L.ccs_field_enable(self._h, 1 if on else 0), "ccs_field_enable")
 
     def field_eval(self, site, pos, path=0):
-        """(u, f, exact) of the learned field at pos (n x 3); path 0 tensor cores, 1 warp."""
+        """(u (n, k), g (n, k, 3), exact) of the k fields site `site` uses at pos (n x 3):
+        values and minus their gradients; path 0 tensor cores, 1 warp."""
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
         n = pos.shape[0]
-        u = np.empty(n)
-        f = np.empty((n, 3))
+        u = np.zeros((n, 4))
+        g = np.zeros((n, 4, 3))
         ex = np.empty(n, dtype=np.int8)
-        self._check(self._L.ccs_field_eval(self._h, n, site, _p(pos), path, _p(u), _p(f), _p(ex)), "ccs_field_eval")
-        return u, f, ex
+        k = ctypes.c_int32()
+        self._check(self._L.ccs_field_eval(self._h, n, site, _p(pos), path, _p(u), _p(g), _p(ex), ctypes.byref(k)),
+                    "ccs_field_eval")
+        return u[:, :k.value], g[:, :k.value], ex
 
     def _field_sizes(self):
         nt = 16 * (1 << self.field_log2) * 2
@@ -317,17 +324,20 @@ class Engine:
         return nt, nm
 
     def field_get_weights(self):
+        """(table [16][T][2], mlp vector, scales: nf output then nf gradient scales)."""
         nt, nm = self._field_sizes()
         t = np.empty(nt, dtype=np.float32)
         m = np.empty(nm, dtype=np.float32)
-        s = ctypes.c_double()
-        self._check(self._L.ccs_field_get_weights(self._h, _p(t), _p(m), ctypes.byref(s)), "ccs_field_get_weights")
-        return t.reshape(16, -1, 2), m, s.value
+        s = np.empty(2 * self.field_nf)
+        self._check(self._L.ccs_field_get_weights(self._h, _p(t), _p(m), _p(s)), "ccs_field_get_weights")
+        return t.reshape(16, -1, 2), m, s
 
-    def field_set_weights(self, table, mlp, scale):
+    def field_set_weights(self, table, mlp, scales):
         t = np.ascontiguousarray(table, dtype=np.float32)
         m = np.ascontiguousarray(mlp, dtype=np.float32)
-        self._check(self._L.ccs_field_set_weights(self._h, _p(t), _p(m), float(scale)), "ccs_field_set_weights")
+        sc = np.ascontiguousarray(scales, dtype=np.float64)
+        assert sc.shape == (2 * self.field_nf,)
+        self._check(self._L.ccs_field_set_weights(self._h, _p(t), _p(m), _p(sc)), "ccs_field_set_weights")
 
     def field_loss_grad(self, pos, labels):
         """Mean loss and its gradients (table [16][T][2], mlp vector) on the given samples."""
@@ -340,6 +350,13 @@ class Engine:
         self._check(self._L.ccs_field_loss_grad(self._h, pos.shape[0], _p(pos), _p(lab), ctypes.byref(loss),
                                                 _p(dt), _p(dm)), "ccs_field_loss_grad")
         return loss.value, dt.reshape(16, -1, 2), dm
+
+    def field_labels(self, pos):
+        """The far-part labels (n, nf, 4): value and minus the gradient of every field."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        out = np.empty((pos.shape[0], self.field_nf, 4))
+        self._check(self._L.ccs_field_labels(self._h, pos.shape[0], _p(pos), _p(out)), "ccs_field_labels")
+        return out
 
     def eval_site_forces(self, site, pos, want_visits=True):
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)

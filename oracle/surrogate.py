@@ -242,3 +242,73 @@ def adam_step(p, g, m, v, t, lr, b1=0.9, b2=0.99, eps=1e-15):
     mh = m / (1 - b1 ** t)
     vh = v / (1 - b2 ** t)
     p -= lr * mh / (np.sqrt(vh) + eps)
+
+
+KCOUL = 332.06348078020324
+
+
+def field_layout(gas, coul_on, dip_on):
+    """The engine's fields for a gas (ccs_gas numbering): a list of
+    (kind, lj, q, comp) -- kind 0 the far potential of a site type with LJ
+    parameter set lj (0 none, 1 primary, 2 carbon) and charge q, kind 1
+    component comp of the far electric field -- and the field of each site
+    and the dipole's site."""
+    if gas == 2:    # N2: N, N, central charge
+        fields = [(0, 1, -0.4825 if coul_on else 0.0, 0), (0, 0, 0.965 if coul_on else 0.0, 0)]
+        site_field, dip = [0, 0, 1], (2 if dip_on else -1)
+    elif gas == 3:  # CO2: O, C, O
+        fields = [(0, 1, -0.3256 if coul_on else 0.0, 0), (0, 2, 0.6512 if coul_on else 0.0, 0)]
+        site_field, dip = [0, 1, 0], (1 if dip_on else -1)
+    else:
+        fields = [(0, 1, 0.0, 0)]
+        site_field, dip = [0], (0 if dip_on else -1)
+    if dip >= 0:
+        fields += [(1, 0, 0.0, a) for a in range(3)]
+    return fields, site_field, dip
+
+
+def far_fields(pts, xyz, q, ab, abc, fields, lj_cutoff, coul_cutoff, r_in, r_out, coul_on):
+    """Far parts of the range-separated pair terms at points (n, 3): for each
+    field its value and minus its gradient, (n, nf, 4).  Far weight 1 - S(r)
+    (switch); LJ shifted at lj_cutoff (Force.cpp:83-102), Coulomb and the
+    dipole's field in the shifted-force form within coul_cutoff
+    (Force.cpp:671-683, 393-426).  ab / abc: (natoms, 2) pair coefficients
+    A = 4 eps sig^12, B = 4 eps sig^6 of the primary and carbon sets."""
+    pts = np.atleast_2d(np.asarray(pts, dtype=np.float64))
+    out = np.zeros((len(pts), len(fields), 4))
+    rl, rc = lj_cutoff, coul_cutoff
+    rc6i, rc3i = 1.0 / rl ** 6, 1.0 / rc ** 3
+    for i, p in enumerate(pts):
+        d = p[None, :] - xyz
+        r2 = (d * d).sum(1)
+        r = np.sqrt(r2)
+        S, dS = switch(r, r_in, r_out)
+        wf, dsr = 1.0 - S, dS / r
+        in_lj, in_c = r2 < rl * rl, r2 < rc * rc
+        ir2 = 1.0 / r2
+        ir6 = ir2 ** 3
+        for f, (kind, lj, qs, comp) in enumerate(fields):
+            if kind == 0:
+                u = np.zeros_like(r)
+                fs = np.zeros_like(r)
+                if lj:
+                    A, B = (ab if lj == 1 else abc).T
+                    u += np.where(in_lj, ir6 * (A * ir6 - B) - (A * rc6i * rc6i - B * rc6i), 0.0)
+                    fs += np.where(in_lj, ir6 * (12 * A * ir6 - 6 * B) * ir2, 0.0)
+                if qs != 0.0 and coul_on:
+                    kq = KCOUL * qs * q
+                    u += np.where(in_c, kq * (1 / r - 1.5 / rc + 0.5 * r2 * rc3i), 0.0)
+                    fs += np.where(in_c, kq * (1 / r ** 3 - rc3i), 0.0)
+                fsc = wf * fs + u * dsr
+                out[i, f, 0] = (wf * u).sum()
+                out[i, f, 1:] = (fsc[:, None] * d).sum(0)
+            else:
+                sq = np.where(in_c, q * (1 / r ** 3 - rc3i), 0.0)
+                tq = np.where(in_c, -3 * q / r ** 5, 0.0)
+                da = d[:, comp]
+                out[i, f, 0] = (wf * sq * da).sum()
+                t2 = wf * tq * da - sq * da * dsr
+                g = (t2[:, None] * d).sum(0)
+                g[comp] += (wf * sq).sum()
+                out[i, f, 1:] = -g
+    return out

@@ -1,5 +1,5 @@
 """The learned field on the GPU against its CPU restatement and against the
-exact evaluator (GPU, through the C-ABI).
+exact far-part labels (GPU, through the C-ABI).
 
 Bars (stated here, used below):
   training gradients: the GPU's loss and every gradient of the
@@ -7,15 +7,21 @@ Bars (stated here, used below):
     FP64 restatement (oracle/surrogate.py) on the same parameters and
     samples: max |difference| <= 2e-3 of the largest gradient entry;
   inference: both GPU paths (tcgen05 tiles of the lane pass, warp path of
-    the warp pass) against the restatement's bfloat16 arithmetic: potential
-    and force within 1e-2 of their RMS on >= 99 % of positions (a bf16
-    rounding that tips the other way at a hidden unit moves one term by
-    2^-8), and the two paths within the same bar of each other;
-  training: deterministic for a seed (identical parameters twice), loss
-    falls at least tenfold, and the trained field's forces outside the exact
-    zone agree with the exact evaluator to a median relative error <= 5 %;
+    the warp pass) against the restatement's bfloat16 arithmetic, every
+    field a site uses: value and gradient within 1e-2 of their RMS on
+    >= 99 % of positions (a bf16 rounding that tips the other way at a hidden
+    unit moves one term by 2^-8), and the two paths within the same bar of
+    each other;
+  labels: the GPU's far-part labels (FP32 terms, FP64 sums) against the FP64
+    restatement: within 2e-4 of each field's RMS (value and gradient);
+  training: deterministic for a seed (identical parameters twice), loss falls
+    at least tenfold, and the trained far fields agree with fresh labels:
+    median gradient error <= 5 % of the gradient RMS per field;
   exact zone: every position within the fallback radius of an atom is
-    evaluated exactly.
+    evaluated exactly;
+  trajectories: with the field, status agreement with the plain FP32 run
+    >= 95 % and the paired CCS within 1 % (the 0.5 % bar of the task is
+    checked on the 20,000-atom workload by bench.py's accuracy report).
 """
 import os
 
@@ -34,6 +40,27 @@ def _system(kind, tmp, n=2000):
     return host.System(p)
 
 
+def _pair_coefficients(S):
+    """Target and its pair coefficients A = 4 eps sig^12, B = 4 eps sig^6 (primary
+    set; the carbon set for CO2, else the primary one again)."""
+    t = S.target()
+    ab = np.stack([4 * t["eps"] * t["sig"] ** 12, 4 * t["eps"] * t["sig"] ** 6], 1)
+    abc = ab
+    if S.info["gas_flag"] == 3:
+        abc = np.stack([4 * t["eps_c"] * t["sig_c"] ** 12, 4 * t["eps_c"] * t["sig_c"] ** 6], 1)
+    return t, ab, abc
+
+
+def _site_fields(S, nf):
+    """The fields each site of the gas uses: its type's far potential, then
+    the three far-field components at the dipole's site."""
+    from oracle.surrogate import field_layout
+    base, site_field, dip = field_layout(S.info["gas_flag"], True, False)
+    dip_on = nf > len(base)
+    _, site_field, dip = field_layout(S.info["gas_flag"], True, dip_on)
+    return [[f] + ([nf - 3, nf - 2, nf - 1] if s == dip else []) for s, f in enumerate(site_field)]
+
+
 def _random_field(S, log2_table=14, base=8, finest=256, seed=1):
     """A context whose field has random (non-trivial) parameters, and the
     restatement holding the same parameters."""
@@ -41,24 +68,26 @@ def _random_field(S, log2_table=14, base=8, finest=256, seed=1):
     eng = S.engine(precision=0)
     rep = eng.field_setup(log2_table=log2_table, base_res=base, finest_res=finest)
     t, m, _ = eng.field_get_weights()
+    nf = rep["nfields"]
     rng = np.random.default_rng(seed)
     t = rng.normal(0, 0.5, size=t.shape).astype(np.float32)
     m = (m + rng.normal(0, 0.05, size=m.shape)).astype(np.float32)
-    eng.field_set_weights(t, m, 0.8)
+    scales = np.concatenate([rng.uniform(0.5, 2.0, nf), rng.uniform(0.5, 2.0, nf)])
+    eng.field_set_weights(t, m, scales)
     lo = np.array(rep["domain_lo"])
     side = rep["domain_side"]
-    F = Field(lo, lo + side, hidden=64, outputs=rep["nfields"], scale=0.8, levels=16, log2_table=log2_table,
+    F = Field(lo, lo + side, hidden=64, outputs=nf, scale=scales[:nf], levels=16, log2_table=log2_table,
               features=2, base=base, finest=finest)
     F.grid.res = np.array(rep["res"], dtype=np.int64)
     F.grid.table = t.astype(np.float64)
     F.set_mlp_vector(m.astype(np.float64))
-    return eng, F, lo, side, rng
+    return eng, F, scales, lo, side, rng
 
 
 @pytest.mark.parametrize("kind", ["globule_n2", "c60_he"])
 def test_loss_gradients_match_oracle(tmp_path, kind):
     S = _system(kind, str(tmp_path))
-    eng, F, lo, side, rng = _random_field(S)
+    eng, F, scales, lo, side, rng = _random_field(S)
     nf = F.W3.shape[0]
     n = 256
     x = (lo + side * (0.3 + 0.4 * rng.random((n, 3)))).astype(np.float32).astype(np.float64)
@@ -66,7 +95,7 @@ def test_loss_gradients_match_oracle(tmp_path, kind):
     Fs = rng.normal(size=(n, nf, 3))
     lab = np.concatenate([U[:, :, None], Fs], axis=2)
     loss, dt, dm = eng.field_loss_grad(x, lab)
-    lo_, dto, dmo = F.loss_and_grad(x, U, Fs)
+    lo_, dto, dmo = F.loss_and_grad(x, U, Fs, lam_u=0.1, u0=0.05 * scales[:nf], f0=0.05 * scales[nf:])
     assert abs(loss - lo_) <= 1e-4 * abs(lo_)
     assert np.abs(dm - dmo).max() <= 2e-3 * np.abs(dmo).max()
     assert np.abs(dt - dto).max() <= 2e-3 * np.abs(dto).max()
@@ -76,22 +105,54 @@ def test_loss_gradients_match_oracle(tmp_path, kind):
 @pytest.mark.parametrize("kind", ["globule_n2", "c60_he"])
 def test_inference_paths_match_oracle(tmp_path, kind):
     S = _system(kind, str(tmp_path))
-    eng, F, lo, side, rng = _random_field(S, seed=2)
+    eng, F, scales, lo, side, rng = _random_field(S, seed=2)
     x = lo + side * (0.3 + 0.4 * rng.random((2000, 3)))
     ub, Fb = F.infer_bf16(x)
-    sites = [0, 2] if F.W3.shape[0] == 2 else [0]
-    for site in sites:
-        fld = 0 if site == 0 else 1
-        ur = np.sqrt((ub[:, fld] ** 2).mean())
-        fr = np.sqrt((np.linalg.norm(Fb[:, fld], axis=1) ** 2).mean())
+    for site, fl in enumerate(_site_fields(S, F.W3.shape[0])):
         out = {}
         for path in (0, 1):
-            u, f, _ = eng.field_eval(site, x, path=path)
-            out[path] = (u, f)
-            assert (np.abs(u - ub[:, fld]) <= 1e-2 * ur).mean() >= 0.99, (path, site)
-            assert (np.linalg.norm(f - Fb[:, fld], axis=1) <= 1e-2 * fr).mean() >= 0.99, (path, site)
-        assert (np.abs(out[0][0] - out[1][0]) <= 1e-2 * ur).mean() >= 0.99
-        assert (np.linalg.norm(out[0][1] - out[1][1], axis=1) <= 1e-2 * fr).mean() >= 0.99
+            u, g, _ = eng.field_eval(site, x, path=path)
+            out[path] = (u, g)
+        assert out[0][0].shape[1] == len(fl)
+        for k, f in enumerate(fl):
+            ur = np.sqrt((ub[:, f] ** 2).mean())
+            gr = np.sqrt((np.linalg.norm(Fb[:, f], axis=1) ** 2).mean())
+            for path in (0, 1):
+                u, g = out[path]
+                assert (np.abs(u[:, k] - ub[:, f]) <= 1e-2 * ur).mean() >= 0.99, (path, site, f)
+                assert (np.linalg.norm(g[:, k] - Fb[:, f], axis=1) <= 1e-2 * gr).mean() >= 0.99, (path, site, f)
+            assert (np.abs(out[0][0][:, k] - out[1][0][:, k]) <= 1e-2 * ur).mean() >= 0.99
+            assert (np.linalg.norm(out[0][1][:, k] - out[1][1][:, k], axis=1) <= 1e-2 * gr).mean() >= 0.99
+    eng.close()
+
+
+def _probe_points(S, n, rng, rmin=3.5, rmax=14.0):
+    t = S.target()
+    a = rng.integers(0, len(t["x"]), n)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return np.stack([t["x"][a], t["y"][a], t["z"][a]], 1) + d * rng.uniform(rmin, rmax, (n, 1))
+
+
+def test_labels_match_oracle(tmp_path):
+    from oracle.surrogate import far_fields, field_layout
+    S = _system("globule_n2", str(tmp_path))
+    eng = S.engine(precision=0)
+    rep = eng.field_setup()
+    p = S.params()
+    t, ab, abc = _pair_coefficients(S)
+    fields, _, _ = field_layout(2, True, True)
+    x = _probe_points(S, 300, np.random.default_rng(3))
+    got = eng.field_labels(x)
+    xyz = np.stack([t["x"], t["y"], t["z"]], 1)
+    ref = far_fields(x.astype(np.float32).astype(np.float64), xyz, t["q"], ab, abc, fields, p.lj_cutoff,
+                     p.coul_cutoff, 6.0, 8.0, True)
+    assert got.shape == ref.shape == (300, 5, 4)
+    for f in range(5):
+        vr = np.sqrt((ref[:, f, 0] ** 2).mean())
+        gr = np.sqrt((np.linalg.norm(ref[:, f, 1:], axis=1) ** 2).mean())
+        assert np.abs(got[:, f, 0] - ref[:, f, 0]).max() <= 2e-4 * vr, f
+        assert np.linalg.norm(got[:, f, 1:] - ref[:, f, 1:], axis=1).max() <= 2e-4 * gr, f
     eng.close()
 
 
@@ -111,23 +172,20 @@ def test_training_is_deterministic_and_fits(tmp_path):
     assert reps[0]["final_loss"] < 0.1 * reps[0]["first_loss"], reps[0]
 
 
-def test_trained_field_forces_match_the_exact_evaluator(tmp_path):
+def test_trained_field_matches_fresh_labels(tmp_path):
     S = _system("globule_n2", str(tmp_path))
     eng = S.engine(precision=0)
     rep = eng.field_train(**SMALL)
-    rng = np.random.default_rng(5)
-    t = S.target()
-    a = rng.integers(0, len(t["x"]), 4000)
-    d = rng.normal(size=(4000, 3))
-    d /= np.linalg.norm(d, axis=1, keepdims=True)
-    x = np.stack([t["x"][a], t["y"][a], t["z"][a]], 1) + d * rng.uniform(3.5, 12.0, (4000, 1))
-    for site in (0, 2):
-        u, f, ex = eng.field_eval(site, x, path=0)
-        fe, Ue, _ = eng.eval_site_forces(site, x)
+    x = _probe_points(S, 4000, np.random.default_rng(5))
+    lab = eng.field_labels(x)
+    for site, fl in enumerate(_site_fields(S, rep["nfields"])):
+        u, g, ex = eng.field_eval(site, x, path=0)
         use = ex == 0
         assert use.mean() > 0.5
-        rel = np.linalg.norm(f - fe, axis=1)[use] / (np.linalg.norm(fe, axis=1)[use] + 0.05)
-        assert np.median(rel) <= 0.05, (site, np.median(rel), rep)
+        for k, f in enumerate(fl):
+            gr = np.sqrt((np.linalg.norm(lab[use, f, 1:], axis=1) ** 2).mean())
+            err = np.linalg.norm(g[use, k] - lab[use, f, 1:], axis=1) / gr
+            assert np.median(err) <= 0.05, (f, np.median(err), rep)
     eng.close()
 
 
@@ -135,12 +193,24 @@ def test_positions_near_atoms_are_exact(tmp_path):
     S = _system("globule_n2", str(tmp_path))
     eng = S.engine(precision=0)
     eng.field_setup()
-    rng = np.random.default_rng(6)
-    t = S.target()
-    a = rng.integers(0, len(t["x"]), 3000)
-    d = rng.normal(size=(3000, 3))
-    d /= np.linalg.norm(d, axis=1, keepdims=True)
-    x = np.stack([t["x"][a], t["y"][a], t["z"][a]], 1) + d * rng.uniform(0.0, 3.0, (3000, 1))
+    x = _probe_points(S, 3000, np.random.default_rng(6), 0.0, 3.0)
     _, _, ex = eng.field_eval(0, x, path=1)
     assert ex.all()
     eng.close()
+
+
+def test_field_trajectories_paired_with_plain(tmp_path):
+    S = _system("globule_n2", str(tmp_path), n=4000)
+    rnd = S.predraw(4000)
+    eng = S.engine(precision=0)
+    plain = eng.run(rnd)
+    eng.field_train(samples=1000000, iterations=1500, batch=32768)
+    eng.field_enable(True)
+    fld = eng.run(rnd)
+    eng.close()
+    assert (fld["status"] == plain["status"]).mean() >= 0.95
+    bmax = S.info["bmax"]
+    a = np.pi * np.where(plain["status"] == 1, plain["one_minus_cos"], 0.0) * bmax ** 2
+    b = np.pi * np.where(fld["status"] == 1, fld["one_minus_cos"], 0.0) * bmax ** 2
+    ok = (plain["status"] <= 1) & (fld["status"] <= 1)
+    assert abs((b - a)[ok].mean()) <= 0.01 * a[ok].mean()

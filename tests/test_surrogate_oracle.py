@@ -116,3 +116,22 @@ def test_adam_fit_lowers_the_loss():
         adam_step(v, dm, mv, vv, t, 1e-2)
         f.set_mlp_vector(v)
     assert loss < 0.1 * first, (first, loss)
+
+
+def test_far_fields_are_minus_their_gradients():
+    """The far parts of the range-separated pair terms (the training labels):
+    every field's second entry is minus the gradient of its value."""
+    from oracle.surrogate import far_fields, field_layout
+    rng = np.random.default_rng(8)
+    xyz = rng.normal(size=(60, 3)) * 4
+    q = rng.normal(size=60) * 0.3
+    ab = np.tile([4 * 0.1 * 3.3 ** 12, 4 * 0.1 * 3.3 ** 6], (60, 1))
+    for gas in (2, 3, 1):
+        fields, _, _ = field_layout(gas, True, True)
+        args = (xyz, q, ab, ab * 1.1, fields, 12.0, 25.0, 6.0, 8.0, True)
+        for p in (np.array([[9.0, 1.0, -2.0]]), np.array([[0.5, 7.1, 3.0]])):
+            o = far_fields(p, *args)
+            h = 1e-5
+            for a in range(3):
+                fd = (far_fields(p + h * np.eye(3)[a], *args)[0, :, 0] - far_fields(p - h * np.eye(3)[a], *args)[0, :, 0]) / (2 * h)
+                np.testing.assert_allclose(o[0, :, 1 + a], -fd, rtol=1e-6, atol=1e-9)
