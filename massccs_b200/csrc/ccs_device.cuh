@@ -90,6 +90,7 @@ struct KParams {
   unsigned long long *park_next;    // next parked trajectory to resume
   unsigned long long park_cap;
   uint32_t park_steps;
+  int lcap;                         // warp pass: candidate-list entries (dynamic shared memory)
   // batched ions: per-ion parameters (their rnd/status/omc/steps/visits point
   // at the ion's first trajectory) and the global index of each ion's first
   // trajectory (nions + 1 entries); unused by single-ion runs
@@ -580,7 +581,9 @@ __device__ __forceinline__ void reduce_group_row(const Acc<T, GasShape<GAS>::NS>
   }
 }
 
-constexpr int LCAP = 2048;  // candidate-list entries kept in shared memory per CTA
+constexpr int LCAP = 2048;  // least candidate-list entries kept in shared memory per CTA (the
+                            // launch's kp.lcap, sized to the target's densest sphere, can be more)
+constexpr int LCAP_MAX = 8192;
 constexpr float LSKIN = 1.0f;  // A: the list's margin; reused while the probe moves less
 
 // Block-wide exclusive scan of len; total receives the block sum.  Ends
@@ -637,8 +640,8 @@ template <typename T, int GAS> struct ProbeSites {
 template <typename T, int NT, int GAS, bool HASQ, bool SPLIT = false>
 __device__ __noinline__ Acc<T, GasShape<GAS>::NS> chunked_visits(const KParams *__restrict__ kpg,
                                                                  const ProbeSites<T, GAS> ps, T cx, T cy, T cz,
-                                                                 T R, int tid, int *sm_list, int *sm_wsum,
-                                                                 uint32_t *nvis_out) {
+                                                                 T R, int tid, int *sm_list, int lcap,
+                                                                 int *sm_wsum, uint32_t *nvis_out) {
   const KParams &kp = *kpg;
   const int lane = tid & 31, w = tid >> 5;
   Acc<T, GasShape<GAS>::NS> acc;
@@ -651,12 +654,12 @@ __device__ __noinline__ Acc<T, GasShape<GAS>::NS> chunked_visits(const KParams *
     int b, len, total;
     column_run(kp, base + tid, ncol, i0, j0, nj, inv_nj, cx, cy, cz, R, b, len);
     const int excl = block_excl_scan<NT>(len, lane, w, sm_wsum, total);
-    for (int cs = 0; cs < total; cs += LCAP) {
-      // this thread's run, as far as it falls into the chunk [cs, cs + LCAP)
-      const int lo = max(excl, cs), hi = min(excl + len, cs + LCAP);
+    for (int cs = 0; cs < total; cs += lcap) {
+      // this thread's run, as far as it falls into the chunk [cs, cs + lcap)
+      const int lo = max(excl, cs), hi = min(excl + len, cs + lcap);
       for (int q = lo; q < hi; q++) sm_list[q - cs] = b + (q - excl);
       __syncthreads();
-      visit_list<T, NT, GAS, HASQ, SPLIT>(kp, ps.p, ps.act, sm_list, min(LCAP, total - cs), tid, acc);
+      visit_list<T, NT, GAS, HASQ, SPLIT>(kp, ps.p, ps.act, sm_list, min(lcap, total - cs), tid, acc);
       __syncthreads();  // the chunk is rewritten next
     }
     if (total == 0) __syncthreads();  // sm_wsum is rewritten next (block-uniform branch)
@@ -676,13 +679,13 @@ __device__ __noinline__ Acc<T, GasShape<GAS>::NS> chunked_visits(const KParams *
 // run lengths.  While the probe's centre stays within LSKIN of where the list
 // was built, the sphere of the current step lies inside the list's sphere, so
 // the list is reused as is; the per-site cutoff tests then pick exactly the
-// pairs the reference sums.  A list longer than LCAP is not kept: such steps
+// pairs the reference sums.  A list longer than lcap is not kept: such steps
 // flatten the runs of the reach sphere chunk by chunk.
 //
 // The sums are reduced per warp with a reduce-scatter butterfly and then
 // across warps in shared memory in a fixed order, so every thread ends with
 // identical bits.  All threads call this with identical arguments.
-//   sm_list: LCAP ints; sm_wsum: NT/32 ints; sm_red: (NT/32 + 1) * RedShape<GAS>::P values
+//   sm_list: lcap ints; sm_wsum: NT/32 ints; sm_red: (NT/32 + 1) * RedShape<GAS>::P values
 //   list_n, list_c: the CTA's list state (list_n < 0: no valid list)
 //   SPLIT: the near part of the range separation (candidates within r_out);
 //   the raw sums (per site f and U, then E and its gradient) go to raw[] and
@@ -692,7 +695,7 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
                                                   const bool (&act)[GasShape<GAS>::NS], const T (&cen)[3],
                                                   T off, T (&f)[GasShape<GAS>::NS][3],
                                                   T (&U)[GasShape<GAS>::NS], uint32_t &visits, int tid,
-                                                  int *sm_list, int *sm_wsum, T *sm_red, int &list_n,
+                                                  int *sm_list, int lcap, int *sm_wsum, T *sm_red, int &list_n,
                                                   T (&list_c)[3], const KParams *__restrict__ kpg,
                                                   T *raw = nullptr) {
   constexpr int NS = GasShape<GAS>::NS;
@@ -734,12 +737,12 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
           int b, len, total;
           column_run(kp, base + tid, ncol, i0, j0, nj, inv_nj, cx, cy, cz, RL, b, len);
           const int excl = block_excl_scan<NT>(len, lane, w, sm_wsum, total);
-          if (filled + total <= LCAP)
+          if (filled + total <= lcap)
             for (int q = 0; q < len; q++) sm_list[filled + excl + q] = b + q;
           filled += total;
           __syncthreads();  // the runs are in place; sm_wsum may be rewritten
         }
-        list_n = filled <= LCAP ? filled : -1;
+        list_n = filled <= lcap ? filled : -1;
         list_c[0] = cx; list_c[1] = cy; list_c[2] = cz;
       }
       if (list_n >= 0) {
@@ -754,7 +757,7 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
           for (int k = 0; k < 3; k++) ps.p[s][k] = p[s][k];
         }
         uint32_t nc = 0;
-        acc = chunked_visits<T, NT, GAS, HASQ, SPLIT>(kpg, ps, cx, cy, cz, R, tid, sm_list, sm_wsum, &nc);
+        acc = chunked_visits<T, NT, GAS, HASQ, SPLIT>(kpg, ps, cx, cy, cz, R, tid, sm_list, lcap, sm_wsum, &nc);
         nvis += nc;
       }
     }
@@ -1600,7 +1603,8 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
   constexpr int NS = S::NS;
   static_assert(!SURR || (sizeof(T) == 4 && !BATCH), "the learned field runs in FP32 single-ion launches");
   __shared__ float sm_site[NS][4 * FL_SITE_FIELDS];
-  __shared__ int sm_list[LCAP], sm_wsum[NT / 32];
+  extern __shared__ int sm_list[];  // kp.lcap entries (dynamic shared memory)
+  __shared__ int sm_wsum[NT / 32];
   __shared__ T sm_red[(NT / 32 + 1) * RedShape<GAS>::P];
   __shared__ unsigned long long blk[8];
   __shared__ unsigned long long sm_idx;
@@ -1690,7 +1694,7 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
               T raw[RedShape<GAS>::NV];
               if (list_split != 1) { list_n = -1; list_split = 1; }  // the candidate list has this mode's reach
               eval_forces_block<T, NT, GAS, HASQ, true>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
-                                                        tid, sm_list, sm_wsum, sm_red, list_n, list_c, Kg, raw);
+                                                        tid, sm_list, kp.lcap, sm_wsum, sm_red, list_n, list_c, Kg, raw);
               // ... plus the far parts from the network, one warp per site
               for (int s = tid >> 5; s < NS; s += NT / 32) {
                 int fl[FL_SITE_FIELDS];
@@ -1728,7 +1732,7 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
               if (list_split != 0) { list_n = -1; list_split = 0; }
             }
             eval_forces_block<T, NT, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
-                                                  tid, sm_list, sm_wsum, sm_red, list_n, list_c, Kg);
+                                                  tid, sm_list, kp.lcap, sm_wsum, sm_red, list_n, list_c, Kg);
           }
         } else {
 #pragma unroll

@@ -167,6 +167,7 @@ KParams ccs_internal::base_params(const ccs_ctx *c) {
   k.h = c->h; k.inv_h = 1.0 / c->h;
   for (int d = 0; d < 3; d++) { k.bb_lo[d] = c->bb_lo[d]; k.bb_hi[d] = c->bb_hi[d]; }
   k.reach = c->reach;
+  k.lcap = c->lcap;
   k.allpairs = c->allpairs;
   k.coul_on = c->coul_on;
   k.dip_on = c->dip_on;
@@ -259,14 +260,15 @@ int setup_spec(ccs_ctx *c, KParams &k, size_t cap, cudaStream_t s) {
 template <bool BATCH>
 int launch_warp_pass(ccs_ctx *c, KernelFn rfn, int rnt, KParams k, cudaStream_t s) {
   int rper_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, rnt, 0));
+  const size_t dyn = (size_t)k.lcap * sizeof(int);  // the candidate list
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, rnt, dyn));
   const unsigned rgrid = (unsigned)((size_t)std::max(rper_sm, 1) * c->sm_count);
   k.spec_max_parked = 2ull * rgrid;  // measured: 448 parked of 3e5 (60 atoms, He) 1.7x faster, 52,241 (1231 atoms, N2) slower
-  rfn<<<rgrid, rnt, 0, s>>>(k, c->d_kparams);
+  rfn<<<rgrid, rnt, dyn, s>>>(k, c->d_kparams);
   CK(cudaGetLastError());
   if (k.spec_rec) {
     k.spec_phase = 1;
-    rfn<<<rgrid, rnt, 0, s>>>(k, c->d_kparams);
+    rfn<<<rgrid, rnt, dyn, s>>>(k, c->d_kparams);
     CK(cudaGetLastError());
     spec_resolve_kernel<BATCH><<<(unsigned)((k.spec_cap + 255) / 256), 256, 0, s>>>(k);
     CK(cudaGetLastError());
@@ -514,6 +516,7 @@ int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const si
   CK(cudaMemcpy(lead->d_bkp, kv.data(), nions * sizeof(KParams), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(lead->d_bstart, st.data(), (nions + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice));
   KParams k = base_params(lead);
+  for (size_t i = 0; i < nions; i++) k.lcap = std::max(k.lcap, ions[i]->lcap);  // one list size per launch
   k.ntraj = total;
   k.ions = lead->d_bkp;
   k.ion_start = lead->d_bstart;
@@ -706,6 +709,45 @@ int ccs_set_params(ccs_ctx *c, const ccs_params *p) {
   return CCS_OK;
 }
 
+// Warp-pass candidate-list size: the most atoms that the column runs of a
+// list sphere (radius reach + 2.5 A: the skin and a site's offset from the
+// probe centre) can hold around one of up to 256 atoms spread through the
+// target, plus an eighth, rounded up to 256, in [LCAP, LCAP_MAX].  A column
+// run reaches at most a column diagonal beyond the sphere sideways, so an
+// atom counts when (d_xy - h sqrt 2)_+^2 + d_z^2 <= R^2.  Steps with more
+// candidates than the list holds flatten them chunk by chunk.
+static int list_capacity(const ccs_ctx *c, const double *x, const double *y, const double *z,
+                         const std::vector<int> &order, const std::vector<int> &start, const int *dims) {
+  const size_t n = order.size();
+  if (c->allpairs || n <= (size_t)ccs::LCAP) return ccs::LCAP;
+  const double R = c->reach + 2.5, w = c->h * std::sqrt(2.0);
+  const int reach_cells = (int)std::ceil((R + w) / c->h);
+  const size_t samples = std::min<size_t>(256, n);
+  int most = 0;
+  for (size_t t = 0; t < samples; t++) {
+    const int a = order[t * n / samples];
+    const double ax = x[a], ay = y[a], az = z[a];
+    int ci[3];
+    const double v[3] = {ax, ay, az};
+    for (int d = 0; d < 3; d++) ci[d] = std::min(dims[d] - 1, std::max(0, (int)std::floor((v[d] - c->origin[d]) / c->h)));
+    int cnt = 0;
+    for (int i = std::max(0, ci[0] - reach_cells); i <= std::min(dims[0] - 1, ci[0] + reach_cells); i++)
+      for (int j = std::max(0, ci[1] - reach_cells); j <= std::min(dims[1] - 1, ci[1] + reach_cells); j++) {
+        const size_t col = ((size_t)i * dims[1] + j) * dims[2];
+        const int k0 = std::max(0, ci[2] - reach_cells), k1 = std::min(dims[2] - 1, ci[2] + reach_cells);
+        for (int q = start[col + k0]; q < start[col + k1 + 1]; q++) {
+          const int b = order[(size_t)q];
+          const double dx = x[b] - ax, dy = y[b] - ay, dz = z[b] - az;
+          const double e = std::max(0.0, std::sqrt(dx * dx + dy * dy) - w);
+          cnt += e * e + dz * dz <= R * R;
+        }
+      }
+    most = std::max(most, cnt);
+  }
+  const int want = (most + most / 8 + 255) / 256 * 256;
+  return std::min(ccs::LCAP_MAX, std::max(ccs::LCAP, want));
+}
+
 int ccs_set_target(ccs_ctx *c, size_t n, const double *x, const double *y, const double *z,
                    const double *q, const double *eps, const double *sig, const double *eps_c,
                    const double *sig_c) {
@@ -767,6 +809,7 @@ int ccs_set_target(ccs_ctx *c, size_t n, const double *x, const double *y, const
   for (size_t i = 0; i < n; i++) order[(size_t)fill[(size_t)cell[i]]++] = (int)i;
   c->max_cell = 0;
   for (long long k = 0; k < ncell; k++) c->max_cell = std::max(c->max_cell, start[(size_t)k + 1] - start[(size_t)k]);
+  c->lcap = list_capacity(c, x, y, z, order, start, dims);
   // packed atom tables: A = 4 eps sig^12, B = 4 eps sig^6 (the lj2, lj1 of Force.cpp:89-90)
   std::vector<float4> xq32(n);
   std::vector<float2> ab32(n), abc32(p.gas == CCS_GAS_CO2 ? n : 0);
@@ -1233,8 +1276,9 @@ extern "C" int ccs_run_device_noalloc(ccs_ctx *c, size_t n, const double *d_rnd,
   KernelFn rfn = pick_resume(c);
   int rper_sm = 0;
   const int rnt = resume_threads(c);
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, rnt, 0));
-  rfn<<<(unsigned)((size_t)std::max(rper_sm, 1) * c->sm_count), rnt, 0, s>>>(k, kparams);
+  const size_t rdyn = (size_t)k.lcap * sizeof(int);
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, rnt, rdyn));
+  rfn<<<(unsigned)((size_t)std::max(rper_sm, 1) * c->sm_count), rnt, rdyn, s>>>(k, kparams);
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev[7], s));
   CK(cudaEventRecord(c->ev[3], s));

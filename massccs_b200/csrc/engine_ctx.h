@@ -25,6 +25,7 @@ struct ccs_ctx {
   std::string err;
   // engine grid
   int nx = 0, ny = 0, nz = 0, natoms = 0, max_cell = 0;
+  int lcap = 2048;  // warp-pass candidate-list entries (ccs::LCAP .. ccs::LCAP_MAX)
   double h = 0, origin[3] = {0, 0, 0}, bb_lo[3] = {0, 0, 0}, bb_hi[3] = {0, 0, 0}, reach = 0;
   int charged = 0, allpairs = 0, coul_on = 0, dip_on = 0;
   float4 *d_xyzq32 = nullptr;

@@ -1025,8 +1025,8 @@ int ensure_scratch(ccs_ctx *c, FieldState *fs, size_t B) {
 
 constexpr size_t TRAIN_SMEM = (size_t)(2 * FL_H * FL_E + 2 * FL_H * FL_H + 2 * FL_H + FL_NF * FL_H + FL_NF) * sizeof(float);
 
-// Loss gradients of one batch (indices already in fs->bidx) into fs->mgrad
-// and fs->tgrad; the batch's mean loss into *loss_dev.
+// The per-sample pass (forward, backward, table gradients) and the per-chunk
+// weight-gradient partial sums of one batch, for NF fields.
 template <int NF>
 void launch_train(ccs_ctx *c, FieldState *fs, const float4 *pos, const float *lab, int B, int grid, float invB,
                   cudaStream_t s) {
