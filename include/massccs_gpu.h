@@ -251,17 +251,17 @@ int ccs_measure_fp32_peak(int device, double ms, double *tflops);
  * err_threshold.  FP32 precision, force types 2, 4 and 6. */
 typedef struct {
   int64_t samples;          /* training samples (default 4,000,000) */
-  int32_t iterations;       /* Adam steps (default 4000) */
-  int32_t batch;            /* samples per step (default 65536) */
-  int32_t log2_table;       /* rows per level = 2^log2_table (default 18, at most 22) */
-  int32_t base_res;         /* coarsest grid resolution over the domain (default 16) */
-  int32_t finest_res;       /* finest grid resolution (default 2048) */
+  int32_t iterations;       /* Adam steps (default 6000) */
+  int32_t batch;            /* samples per step (default 32768) */
+  int32_t log2_table;       /* rows per level = 2^log2_table (default 20, at most 22) */
+  int32_t base_res;         /* coarsest grid resolution over the domain (default 8) */
+  int32_t finest_res;       /* finest grid resolution (default 128) */
   int32_t validation;       /* validation samples for the error voxels (default 1,048,576) */
   double fallback_radius;   /* A: exact evaluation within this distance of any atom (default 3.0) */
   double voxel;             /* A: edge of the exact-evaluation bitmap's voxels (default 0.5) */
   double err_voxel;         /* A: edge of the validation-error voxels (default 2.0) */
-  double err_threshold;     /* relative force error |F - F*| / (|F*| + f0) above which a voxel is
-                               evaluated exactly (default 0.05) */
+  double err_threshold;     /* force error |G - G*| / g of a field (g: the RMS of its gradient
+                               labels) above which a voxel is evaluated exactly (default 0.1) */
   double near_fraction;     /* share of samples drawn in the shell around atoms (default 0.5) */
   double near_shell;        /* A: that shell's thickness beyond fallback_radius (default 6.0) */
   double lr;                /* Adam learning rate, decayed tenfold over the run (default 1e-2) */
@@ -269,7 +269,7 @@ typedef struct {
                                s and g the RMS of the field's values and gradients
                                (defaults 0.1, 0.05, 0.05) */
   uint64_t seed;            /* sampling, initialisation and batch order (default 2104) */
-  double r_in, r_out;       /* A: the range-separation switch (defaults 6 and 8) */
+  double r_in, r_out;       /* A: the range-separation switch (defaults 6 and 12) */
 } ccs_field_params;
 
 typedef struct {
@@ -282,7 +282,7 @@ typedef struct {
   double sample_ms, label_ms, train_ms, validate_ms;
   double first_loss, final_loss;      /* mean training loss of the first and last steps */
   double val_force_rel_rms;           /* validation: RMS over samples of the largest
-                                         |G - G*| / (|G*| + f0 g) of the fields */
+                                         |G - G*| / g of the fields */
   double val_force_rel_p99;
   double val_u_rel_rms;               /* RMS of the largest |u - U*| / s of the fields */
   double exact_fraction;              /* share of the domain's voxels evaluated exactly */

@@ -1603,7 +1603,7 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
   constexpr int NS = S::NS;
   static_assert(!SURR || (sizeof(T) == 4 && !BATCH), "the learned field runs in FP32 single-ion launches");
   __shared__ float sm_site[NS][4 * FL_SITE_FIELDS];
-  extern __shared__ int sm_list[];  // kp.lcap entries (dynamic shared memory)
+  extern __shared__ int sm_list[];  // kp.lcap entries (+ LCAP with the field; dynamic shared memory)
   __shared__ int sm_wsum[NT / 32];
   __shared__ T sm_red[(NT / 32 + 1) * RedShape<GAS>::P];
   __shared__ unsigned long long blk[8];
@@ -1657,8 +1657,12 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
     const KParams &K = ion_params<BATCH>(kp, L.ion);
     const KParams *Kg = ion_params_ptr<BATCH>(kp, kpg, L.ion);
     int list_n = -1;  // this trajectory's candidate list (none yet)
-    int list_split = -1;  // with the learned field: the list's mode (1: near part of the range separation)
     T list_c[3] = {T(0), T(0), T(0)};
+    // with the learned field, the near part of the range separation keeps a
+    // second list (radius r_out) after the first one's kp.lcap entries, so
+    // steps that move between the exact and the field zone rebuild neither
+    int near_n = -1;
+    T near_c[3] = {T(0), T(0), T(0)};
     for (unsigned it = 1;; it++) {
       int r = S_CONTINUE;
       double omc = 0.0;
@@ -1692,9 +1696,8 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
             if constexpr (SURR) {
               // the switched exact sums over the atoms within r_out ...
               T raw[RedShape<GAS>::NV];
-              if (list_split != 1) { list_n = -1; list_split = 1; }  // the candidate list has this mode's reach
               eval_forces_block<T, NT, GAS, HASQ, true>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
-                                                        tid, sm_list, kp.lcap, sm_wsum, sm_red, list_n, list_c, Kg, raw);
+                                                        tid, sm_list + kp.lcap, LCAP, sm_wsum, sm_red, near_n, near_c, Kg, raw);
               // ... plus the far parts from the network, one warp per site
               for (int s = tid >> 5; s < NS; s += NT / 32) {
                 int fl[FL_SITE_FIELDS];
@@ -1728,9 +1731,6 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
               finish_split<T, GAS, HASQ>(K, raw, ufar, ffar, Ef, Jf, act, fs, Us);
             }
           } else {
-            if constexpr (SURR) {
-              if (list_split != 0) { list_n = -1; list_split = 0; }
-            }
             eval_forces_block<T, NT, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
                                                   tid, sm_list, kp.lcap, sm_wsum, sm_red, list_n, list_c, Kg);
           }
@@ -1799,6 +1799,7 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
       load_init<T, GAS>(L, lane_setup<T, GAS>(Kg, L.j));
       L.mode = M_RESTART;
       list_n = -1;
+      near_n = -1;
     }
     __syncthreads();
   }

@@ -260,7 +260,8 @@ int setup_spec(ccs_ctx *c, KParams &k, size_t cap, cudaStream_t s) {
 template <bool BATCH>
 int launch_warp_pass(ccs_ctx *c, KernelFn rfn, int rnt, KParams k, cudaStream_t s) {
   int rper_sm = 0;
-  const size_t dyn = (size_t)k.lcap * sizeof(int);  // the candidate list
+  // the candidate list (and with the learned field the near-part list)
+  const size_t dyn = (size_t)(k.lcap + (k.field.on ? LCAP : 0)) * sizeof(int);
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rper_sm, (const void *)rfn, rnt, dyn));
   const unsigned rgrid = (unsigned)((size_t)std::max(rper_sm, 1) * c->sm_count);
   k.spec_max_parked = 2ull * rgrid;  // measured: 448 parked of 3e5 (60 atoms, He) 1.7x faster, 52,241 (1231 atoms, N2) slower
@@ -513,8 +514,8 @@ int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const si
     lead->bkp_cap = nions;
   }
   for (size_t i = 0; i < nions; i++) kv[i].deadline = lead->d_work + 8;
-  CK(cudaMemcpy(lead->d_bkp, kv.data(), nions * sizeof(KParams), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(lead->d_bstart, st.data(), (nions + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+  CK(to_dev(lead, lead->d_bkp, kv.data(), nions * sizeof(KParams)));
+  CK(to_dev(lead, lead->d_bstart, st.data(), (nions + 1) * sizeof(unsigned long long)));
   KParams k = base_params(lead);
   for (size_t i = 0; i < nions; i++) k.lcap = std::max(k.lcap, ions[i]->lcap);  // one list size per launch
   k.ntraj = total;
@@ -702,8 +703,9 @@ int ccs_set_params(ccs_ctx *c, const ccs_params *p) {
     dfree(c->d_vtab_v); dfree(c->d_vtab_s);
     CK(cudaMalloc(&c->d_vtab_v, V.size() * sizeof(double)));
     CK(cudaMalloc(&c->d_vtab_s, S.size() * sizeof(double)));
-    CK(cudaMemcpy(c->d_vtab_v, V.data(), V.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->d_vtab_s, S.data(), S.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(to_dev(c, c->d_vtab_v, V.data(), V.size() * sizeof(double)));
+    CK(to_dev(c, c->d_vtab_s, S.data(), S.size() * sizeof(double)));
+    CK(cudaStreamSynchronize(c->stream));  // runs may launch on other streams
     c->vtab_n = (int)V.size();
   }
   return CCS_OK;
@@ -833,24 +835,25 @@ int ccs_set_target(ccs_ctx *c, size_t n, const double *x, const double *y, const
   if (fp64) {
     CK(cudaMalloc(&c->d_xyzq64, n * sizeof(double4)));
     CK(cudaMalloc(&c->d_ab64, n * sizeof(double2)));
-    CK(cudaMemcpy(c->d_xyzq64, xq64.data(), n * sizeof(double4), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->d_ab64, ab64.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(to_dev(c, c->d_xyzq64, xq64.data(), n * sizeof(double4)));
+    CK(to_dev(c, c->d_ab64, ab64.data(), n * sizeof(double2)));
     if (p.gas == CCS_GAS_CO2) {
       CK(cudaMalloc(&c->d_abc64, n * sizeof(double2)));
-      CK(cudaMemcpy(c->d_abc64, abc64.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+      CK(to_dev(c, c->d_abc64, abc64.data(), n * sizeof(double2)));
     }
   } else {
     CK(cudaMalloc(&c->d_xyzq32, n * sizeof(float4)));
     CK(cudaMalloc(&c->d_ab32, n * sizeof(float2)));
-    CK(cudaMemcpy(c->d_xyzq32, xq32.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(c->d_ab32, ab32.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+    CK(to_dev(c, c->d_xyzq32, xq32.data(), n * sizeof(float4)));
+    CK(to_dev(c, c->d_ab32, ab32.data(), n * sizeof(float2)));
     if (p.gas == CCS_GAS_CO2) {
       CK(cudaMalloc(&c->d_abc32, n * sizeof(float2)));
-      CK(cudaMemcpy(c->d_abc32, abc32.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+      CK(to_dev(c, c->d_abc32, abc32.data(), n * sizeof(float2)));
     }
   }
   CK(cudaMalloc(&c->d_cell_start, start.size() * sizeof(int)));
-  CK(cudaMemcpy(c->d_cell_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(to_dev(c, c->d_cell_start, start.data(), start.size() * sizeof(int)));
+  CK(cudaStreamSynchronize(c->stream));  // runs may launch on other streams
   c->have_target = true;
   c->tuned_G = 0;
   c->batch_G = 0;
@@ -1023,7 +1026,7 @@ int ccs_eval_site_forces(ccs_ctx *c, size_t npts, int site, const double *pos, d
   }
   int rc = CCS_OK;
   do {
-    if (cudaMemcpy(dp, pos, npts * 3 * sizeof(double), cudaMemcpyHostToDevice)) { rc = CCS_ERR_CUDA; break; }
+    if (to_dev(c, dp, pos, npts * 3 * sizeof(double))) { rc = CCS_ERR_CUDA; break; }
     KParams k = base_params(c);
     const int G = c->p.lanes_per_traj == 1 ? 1 : c->p.lanes_per_traj == 8 ? 8 : 32;
     ForceFn fn = pick_force(c, G);
@@ -1031,9 +1034,9 @@ int ccs_eval_site_forces(ccs_ctx *c, size_t npts, int site, const double *pos, d
     const size_t grid = std::min<size_t>((npts * G + block - 1) / block, (size_t)c->sm_count * 16);
     fn<<<(unsigned)grid, block, 0, c->stream>>>(k, site, npts, dp, df, dU, dv);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess) { rc = CCS_ERR_CUDA; break; }
-    if (cudaMemcpy(f, df, npts * 3 * sizeof(double), cudaMemcpyDeviceToHost) ||
-        cudaMemcpy(U, dU, npts * sizeof(double), cudaMemcpyDeviceToHost)) { rc = CCS_ERR_CUDA; break; }
-    if (visits && cudaMemcpy(visits, dv, npts * sizeof(uint32_t), cudaMemcpyDeviceToHost)) { rc = CCS_ERR_CUDA; break; }
+    if (to_host(c, f, df, npts * 3 * sizeof(double)) ||
+        to_host(c, U, dU, npts * sizeof(double))) { rc = CCS_ERR_CUDA; break; }
+    if (visits && to_host(c, visits, dv, npts * sizeof(uint32_t))) { rc = CCS_ERR_CUDA; break; }
   } while (0);
   cleanup();
   if (rc) return fail(c, rc, "force evaluation failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1057,7 +1060,7 @@ int ccs_eval_setup(ccs_ctx *c, size_t n, const double *const rnd[9], int8_t *hit
     return fail(c, CCS_ERR_NOMEM, "cudaMalloc for setup");
   }
   for (int k = 0; k < nrows; k++)
-    if (cudaMemcpy(c->d_rnd + (size_t)k * n, rnd[k], n * sizeof(double), cudaMemcpyHostToDevice)) rc = CCS_ERR_CUDA;
+    if (to_dev(c, c->d_rnd + (size_t)k * n, rnd[k], n * sizeof(double))) rc = CCS_ERR_CUDA;
   if (!rc) {
     KParams k = base_params(c);
     k.rnd = c->d_rnd;
@@ -1066,9 +1069,9 @@ int ccs_eval_setup(ccs_ctx *c, size_t n, const double *const rnd[9], int8_t *hit
     setup_kernel<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(k, c->d_status, dpos, dvel);
     if (cudaGetLastError() || cudaStreamSynchronize(c->stream)) rc = CCS_ERR_CUDA;
   }
-  if (!rc && (cudaMemcpy(hit, c->d_status, n, cudaMemcpyDeviceToHost) ||
-              cudaMemcpy(pos, dpos, n * 9 * sizeof(double), cudaMemcpyDeviceToHost) ||
-              cudaMemcpy(vel, dvel, n * 9 * sizeof(double), cudaMemcpyDeviceToHost)))
+  if (!rc && (to_host(c, hit, c->d_status, n) ||
+              to_host(c, pos, dpos, n * 9 * sizeof(double)) ||
+              to_host(c, vel, dvel, n * 9 * sizeof(double))))
     rc = CCS_ERR_CUDA;
   cudaFree(dpos);
   cudaFree(dvel);

@@ -80,7 +80,15 @@ struct ccs_ctx {
 
 namespace ccs_internal {
 
-
+// Copies and fills ordered on the context's stream.  The stream is created
+// non-blocking, so the legacy-stream cudaMemcpy / cudaMemset are not ordered
+// with its kernels (a device memset may still run, and a pageable host-to-
+// device copy may still be in flight, when the next kernel on the stream
+// starts).  Host-to-device copies from pageable memory are staged before the
+// call returns, so the source may be freed; to_host waits for the stream.
+inline cudaError_t to_dev(const ccs_ctx *c, void *dst, const void *src, size_t bytes);
+inline cudaError_t to_host(const ccs_ctx *c, void *dst, const void *src, size_t bytes);
+inline cudaError_t zero_dev(const ccs_ctx *c, void *p, size_t bytes);
 
 inline int fail(ccs_ctx *c, int code, const char *fmt, ...) {
   if (c) {
@@ -126,5 +134,16 @@ int eval_site_forces_device(ccs_ctx *c, size_t npts, int site, const double *d_p
 // The learned field's launch parameters and memory (field.cu).
 void field_kparams(const ccs_ctx *c, ccs::KParams &k);
 void field_free(ccs_ctx *c);
+
+inline cudaError_t to_dev(const ccs_ctx *c, void *dst, const void *src, size_t bytes) {
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+}
+inline cudaError_t to_host(const ccs_ctx *c, void *dst, const void *src, size_t bytes) {
+  const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(c->stream);
+}
+inline cudaError_t zero_dev(const ccs_ctx *c, void *p, size_t bytes) {
+  return cudaMemsetAsync(p, 0, bytes, c->stream);
+}
 
 }  // namespace ccs_internal

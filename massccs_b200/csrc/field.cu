@@ -48,6 +48,7 @@ struct TrainGeo {
   uint32_t tmask;
   int log2t;
   float s[FL_NF];        // output scales
+  float gs[FL_NF];       // RMS gradient of each field's labels
   float u0[FL_NF], f0[FL_NF];  // loss floors of each field's value and gradient
 };
 
@@ -703,9 +704,11 @@ __global__ void __launch_bounds__(TC_ROWS) eval_tc_kernel(FieldK F, size_t n, co
   tc_teardown(tmem);
 }
 
-// Validation: warp inference of every field against the labels; the largest
-// relative force error of each coarse voxel (atomicMax on the float bits:
-// errors are non-negative).
+// Validation: warp inference of every field against the labels.  A sample's
+// force error is the largest over the fields of |F - F*| in units of that
+// field's RMS label gradient, its value error |u - u*| in units of the
+// field's output scale; each coarse voxel keeps the largest force error of its
+// samples (atomicMax on the float bits: errors are non-negative).
 __global__ void validate_kernel(FieldK F, size_t n, const float4 *__restrict__ pos, const float *__restrict__ lab,
                                 int nf, TrainGeo G, float evox_inv, int ev, float *err_f, float *err_u,
                                 unsigned int *vox_err) {
@@ -726,8 +729,7 @@ __global__ void validate_kernel(FieldK F, size_t n, const float4 *__restrict__ p
         const int fld = fl[k];
         const float *lb = lab + (i * nf + fld) * 4;
         const float dx = ff[k][0] - lb[1], dy = ff[k][1] - lb[2], dz = ff[k][2] - lb[3];
-        const float fn = sqrtf(lb[1] * lb[1] + lb[2] * lb[2] + lb[3] * lb[3]);
-        emax = fmaxf(emax, sqrtf(dx * dx + dy * dy + dz * dz) / (fn + G.f0[fld]));
+        emax = fmaxf(emax, sqrtf(dx * dx + dy * dy + dz * dz) / fmaxf(G.gs[fld], 1e-30f));
         eu = fmaxf(eu, fabsf(uu[k] - lb[0]) / fmaxf(G.s[fld], 1e-30f));
       }
     }
@@ -793,6 +795,7 @@ void free_state(FieldState *fs) {
 void refresh_geo(FieldState *fs) {
   for (int f = 0; f < FL_NF; f++) {
     fs->geo.s[f] = (float)fs->s[f];
+    fs->geo.gs[f] = (float)fs->gs[f];
     fs->geo.u0[f] = (float)(fs->p.u0 * fs->s[f]);
     fs->geo.f0[f] = (float)(fs->p.f0 * fs->gs[f]);
   }
@@ -910,17 +913,17 @@ int setup_geometry(ccs_ctx *c, FieldState *fs, const ccs_field_params &p) {
   for (int i = 0; i < FL_H * FL_E; i++) m0[MO_W1 + i] = (float)(normal() * std::sqrt(2.0 / FL_E));
   for (int i = 0; i < FL_H * FL_H; i++) m0[MO_W2 + i] = (float)(normal() * std::sqrt(2.0 / FL_H));
   for (int i = 0; i < FL_NF * FL_H; i++) m0[MO_W3 + i] = (float)(normal() * std::sqrt(1.0 / FL_H));
-  CK(cudaMemcpy(fs->table, t0.data(), nt * sizeof(float2), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(fs->mlp, m0.data(), NM * sizeof(float), cudaMemcpyHostToDevice));
-  CK(cudaMemset(fs->tm, 0, nt * sizeof(float2)));
-  CK(cudaMemset(fs->tv, 0, nt * sizeof(float2)));
-  CK(cudaMemset(fs->tgrad, 0, nt * 2 * sizeof(unsigned long long)));
-  CK(cudaMemset(fs->mm, 0, NM * sizeof(float)));
-  CK(cudaMemset(fs->mv, 0, NM * sizeof(float)));
+  CK(to_dev(c, fs->table, t0.data(), nt * sizeof(float2)));
+  CK(to_dev(c, fs->mlp, m0.data(), NM * sizeof(float)));
+  CK(zero_dev(c, fs->tm, nt * sizeof(float2)));
+  CK(zero_dev(c, fs->tv, nt * sizeof(float2)));
+  CK(zero_dev(c, fs->tgrad, nt * 2 * sizeof(unsigned long long)));
+  CK(zero_dev(c, fs->mm, NM * sizeof(float)));
+  CK(zero_dev(c, fs->mv, NM * sizeof(float)));
   // exact-evaluation bitmap: voxels whose centre is within fallback_radius +
   // half a voxel diagonal of an atom (every point within fallback_radius of an
   // atom then lies in a flagged voxel)
-  CK(cudaMemset(fs->bits, 0, fs->nwords * sizeof(uint32_t)));
+  CK(zero_dev(c, fs->bits, fs->nwords * sizeof(uint32_t)));
   const float R = (float)(p.fallback_radius + 0.5 * std::sqrt(3.0) * p.voxel);
   bitmap_atoms_kernel<<<(c->natoms + 127) / 128, 128, 0, c->stream>>>(c->d_xyzq32, c->natoms, K, (float)p.voxel, R,
                                                                      fs->bits);
@@ -1139,16 +1142,16 @@ void ccs_field_params_default(ccs_field_params *p) {
   if (!p) return;
   std::memset(p, 0, sizeof *p);
   p->samples = 4000000;
-  p->iterations = 4000;
-  p->batch = 65536;
-  p->log2_table = 18;
-  p->base_res = 16;
-  p->finest_res = 2048;
+  p->iterations = 6000;
+  p->batch = 32768;
+  p->log2_table = 20;
+  p->base_res = 8;
+  p->finest_res = 128;
   p->validation = 1 << 20;
   p->fallback_radius = 3.0;
   p->voxel = 0.5;
   p->err_voxel = 2.0;
-  p->err_threshold = 0.05;
+  p->err_threshold = 0.1;
   p->near_fraction = 0.5;
   p->near_shell = 6.0;
   p->lr = 1e-2;
@@ -1157,7 +1160,7 @@ void ccs_field_params_default(ccs_field_params *p) {
   p->f0 = 0.05;
   p->seed = 2104;
   p->r_in = 6.0;
-  p->r_out = 8.0;
+  p->r_out = 12.0;
 }
 
 int ccs_field_setup(ccs_ctx *c, const ccs_field_params *p, ccs_field_report *report) {
@@ -1200,7 +1203,7 @@ int ccs_field_train(ccs_ctx *c, const ccs_field_params *p, ccs_field_report *rep
   rep.samples = (int64_t)fs->nsamples;
   {  // per field: output scale = RMS of its values, gradient scale = RMS of |gradient|
     std::vector<float> lab(fs->nsamples * fs->nf * 4);
-    if (cudaMemcpy(lab.data(), fs->slab, lab.size() * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (to_host(c, lab.data(), fs->slab, lab.size() * sizeof(float)) != cudaSuccess)
       return bail(fail(c, CCS_ERR_CUDA, "label copy"));
     for (int f = 0; f < fs->nf; f++) {
       double su = 0.0, sg = 0.0;
@@ -1239,7 +1242,7 @@ int ccs_field_train(ccs_ctx *c, const ccs_field_params *p, ccs_field_report *rep
   if (rc) { dfree(d_loss); return bail(rc); }
   rep.train_ms = now_ms() - t0;
   float hl[2] = {0.f, 0.f};
-  cudaMemcpy(hl, d_loss, sizeof hl, cudaMemcpyDeviceToHost);
+  to_host(c, hl, d_loss, sizeof hl);
   dfree(d_loss);
   rep.first_loss = hl[0];
   rep.final_loss = p->iterations > 1 ? hl[1] : hl[0];
@@ -1278,9 +1281,9 @@ int ccs_field_train(ccs_ctx *c, const ccs_field_params *p, ccs_field_report *rep
     std::vector<float> hf(nv), hu(nv);
     unsigned long long hc[2] = {0, 0};
     const bool ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(s) == cudaSuccess &&
-                    cudaMemcpy(hf.data(), ef, nv * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess &&
-                    cudaMemcpy(hu.data(), eu, nv * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess &&
-                    cudaMemcpy(hc, cnt, sizeof hc, cudaMemcpyDeviceToHost) == cudaSuccess;
+                    to_host(c, hf.data(), ef, nv * sizeof(float)) == cudaSuccess &&
+                    to_host(c, hu.data(), eu, nv * sizeof(float)) == cudaSuccess &&
+                    to_host(c, hc, cnt, sizeof hc) == cudaSuccess;
     dfree(vpos); dfree(vlab); dfree(ef); dfree(eu); dfree(verr); dfree(cnt);
     if (!ok) return bail(fail(c, CCS_ERR_CUDA, "validation"));
     double sf = 0.0, su = 0.0;
@@ -1300,7 +1303,7 @@ int ccs_field_train(ccs_ctx *c, const ccs_field_params *p, ccs_field_report *rep
     cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s);
     popcount_kernel<<<c->sm_count * 4, 256, 0, s>>>(fs->bits, fs->nwords, cnt);
     unsigned long long hc = 0;
-    cudaMemcpy(&hc, cnt, sizeof hc, cudaMemcpyDeviceToHost);
+    to_host(c, &hc, cnt, sizeof hc);
     dfree(cnt);
     rep.exact_fraction = (double)hc / ((double)fs->k.vx * fs->k.vy * fs->k.vz);
   }
@@ -1342,10 +1345,10 @@ int ccs_field_eval(ccs_ctx *c, size_t n, int site, const double *pos, int path, 
     return rc;
   }
   int herr = 0;
-  bool ok = cudaMemcpy(dp, hp.data(), n * sizeof(float4), cudaMemcpyHostToDevice) == cudaSuccess &&
-            cudaMemset(du, 0, n * 4 * sizeof(double)) == cudaSuccess &&
-            cudaMemset(dg, 0, n * 12 * sizeof(double)) == cudaSuccess &&
-            cudaMemset(derr, 0, sizeof(int)) == cudaSuccess;
+  bool ok = to_dev(c, dp, hp.data(), n * sizeof(float4)) == cudaSuccess &&
+            zero_dev(c, du, n * 4 * sizeof(double)) == cudaSuccess &&
+            zero_dev(c, dg, n * 12 * sizeof(double)) == cudaSuccess &&
+            zero_dev(c, derr, sizeof(int)) == cudaSuccess;
   if (ok) {
     if (path == 0) {
       const size_t tiles = (n + TC_ROWS - 1) / TC_ROWS;
@@ -1356,10 +1359,10 @@ int ccs_field_eval(ccs_ctx *c, size_t n, int site, const double *pos, int path, 
           fs->k, n, dp, site, du, dg, dx);
     }
     ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(c->stream) == cudaSuccess &&
-         cudaMemcpy(u, du, n * 4 * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess &&
-         cudaMemcpy(g, dg, n * 12 * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess &&
-         (!exact || cudaMemcpy(exact, dx, n, cudaMemcpyDeviceToHost) == cudaSuccess) &&
-         cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess;
+         to_host(c, u, du, n * 4 * sizeof(double)) == cudaSuccess &&
+         to_host(c, g, dg, n * 12 * sizeof(double)) == cudaSuccess &&
+         (!exact || to_host(c, exact, dx, n) == cudaSuccess) &&
+         to_host(c, &herr, derr, sizeof(int)) == cudaSuccess;
   }
   cleanup();
   if (!ok) return fail(c, CCS_ERR_CUDA, "field evaluation: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1385,12 +1388,12 @@ int ccs_field_labels(ccs_ctx *c, size_t n, const double *pos, double *labels) {
   KParams kp = base_params(c);
   kp.field = fs->k;
   std::vector<float> hl(n * fs->nf * 4);
-  bool ok = cudaMemcpy(dp, hp.data(), n * sizeof(float4), cudaMemcpyHostToDevice) == cudaSuccess;
+  bool ok = to_dev(c, dp, hp.data(), n * sizeof(float4)) == cudaSuccess;
   if (ok) {
     far_label_kernel<<<(unsigned)std::min<size_t>((n + 7) / 8, (size_t)c->sm_count * 64), 256, 0, c->stream>>>(
         kp, fs->kinds, fs->nf, n, dp, dl);
     ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(c->stream) == cudaSuccess &&
-         cudaMemcpy(hl.data(), dl, hl.size() * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess;
+         to_host(c, hl.data(), dl, hl.size() * sizeof(float)) == cudaSuccess;
   }
   dfree(dp); dfree(dl);
   if (!ok) return fail(c, CCS_ERR_CUDA, "field labels: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1405,10 +1408,10 @@ int ccs_field_get_weights(ccs_ctx *c, float *table, float *mlp, double *scales) 
   if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
   CK(cudaStreamSynchronize(c->stream));
   const size_t nt = (size_t)FL_LEVELS * fs->rows;
-  if (table) CK(cudaMemcpy(table, fs->table, nt * sizeof(float2), cudaMemcpyDeviceToHost));
+  if (table) CK(to_host(c, table, fs->table, nt * sizeof(float2)));
   if (mlp) {
     std::vector<float> m(NM);
-    CK(cudaMemcpy(m.data(), fs->mlp, NM * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(to_host(c, m.data(), fs->mlp, NM * sizeof(float)));
     // external layout: W3 and b3 with nf rows
     std::memcpy(mlp, m.data(), MO_W3 * sizeof(float));
     std::memcpy(mlp + MO_W3, m.data() + MO_W3, fs->nf * FL_H * sizeof(float));
@@ -1428,13 +1431,13 @@ int ccs_field_set_weights(ccs_ctx *c, const float *table, const float *mlp, cons
       if (!(scales[f] > 0)) return fail(c, CCS_ERR_INVALID, "scales must be positive");
   if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, CCS_ERR_CUDA, "cudaSetDevice");
   const size_t nt = (size_t)FL_LEVELS * fs->rows;
-  if (table) CK(cudaMemcpy(fs->table, table, nt * sizeof(float2), cudaMemcpyHostToDevice));
+  if (table) CK(to_dev(c, fs->table, table, nt * sizeof(float2)));
   if (mlp) {
     std::vector<float> m(NM, 0.f);
     std::memcpy(m.data(), mlp, MO_W3 * sizeof(float));
     std::memcpy(m.data() + MO_W3, mlp + MO_W3, fs->nf * FL_H * sizeof(float));
     std::memcpy(m.data() + MO_B3, mlp + MO_W3 + fs->nf * FL_H, fs->nf * sizeof(float));
-    CK(cudaMemcpy(fs->mlp, m.data(), NM * sizeof(float), cudaMemcpyHostToDevice));
+    CK(to_dev(c, fs->mlp, m.data(), NM * sizeof(float)));
   }
   if (scales)
     for (int f = 0; f < fs->nf; f++) { fs->s[f] = scales[f]; fs->gs[f] = scales[fs->nf + f]; }
@@ -1468,24 +1471,24 @@ int ccs_field_loss_grad(ccs_ctx *c, size_t n, const float *pos, const float *lab
     return rc;
   }
   const size_t nt = (size_t)FL_LEVELS * fs->rows;
-  bool ok = cudaMemcpy(dp, hp.data(), n * sizeof(float4), cudaMemcpyHostToDevice) == cudaSuccess &&
-            cudaMemcpy(dl, labels, n * fs->nf * 4 * sizeof(float), cudaMemcpyHostToDevice) == cudaSuccess &&
-            cudaMemcpy(fs->bidx, idx.data(), n * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
-            cudaMemset(fs->tgrad, 0, nt * 2 * sizeof(unsigned long long)) == cudaSuccess;
+  bool ok = to_dev(c, dp, hp.data(), n * sizeof(float4)) == cudaSuccess &&
+            to_dev(c, dl, labels, n * fs->nf * 4 * sizeof(float)) == cudaSuccess &&
+            to_dev(c, fs->bidx, idx.data(), n * sizeof(int)) == cudaSuccess &&
+            zero_dev(c, fs->tgrad, nt * 2 * sizeof(unsigned long long)) == cudaSuccess;
   if (ok) {
     rc = grad_step(c, fs, dp, dl, B, dloss);
     ok = rc == CCS_OK && cudaStreamSynchronize(c->stream) == cudaSuccess;
   }
   float hl = 0.f;
   std::vector<float> m(NM);
-  ok = ok && cudaMemcpy(&hl, dloss, sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess &&
-       cudaMemcpy(m.data(), fs->mgrad, NM * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess;
+  ok = ok && to_host(c, &hl, dloss, sizeof(float)) == cudaSuccess &&
+       to_host(c, m.data(), fs->mgrad, NM * sizeof(float)) == cudaSuccess;
   if (ok && dtable) {
     std::vector<unsigned long long> g(nt * 2);
-    ok = cudaMemcpy(g.data(), fs->tgrad, nt * 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost) == cudaSuccess;
+    ok = to_host(c, g.data(), fs->tgrad, nt * 2 * sizeof(unsigned long long)) == cudaSuccess;
     for (size_t i = 0; ok && i < nt * 2; i++) dtable[i] = (float)((double)(long long)g[i] / FIX_SCALE);
   }
-  if (ok) cudaMemset(fs->tgrad, 0, nt * 2 * sizeof(unsigned long long));
+  if (ok) zero_dev(c, fs->tgrad, nt * 2 * sizeof(unsigned long long));
   cleanup();
   if (!ok) return rc ? rc : fail(c, CCS_ERR_CUDA, "loss gradient: %s", cudaGetErrorString(cudaGetLastError()));
   if (loss) *loss = hl;

@@ -96,9 +96,12 @@ def test_ctypes_layouts_match_the_headers(tmp_path):
 
 
 def test_field_params_defaults(lib):
-    """The learned field's defaults are the stated configuration: 16 levels of
-    2^18 rows, resolutions 16..2048, 4e6 samples, exact within 3 A of an atom."""
+    """The learned field's defaults: 16 levels of 2^20 rows (every level up to
+    resolution 100 dense), resolutions 8..128 over the domain, 4e6 samples,
+    6000 Adam steps, the range-separation switch from 6 to 12 A, exact within
+    3 A of an atom (the measured best of the sweep over table size,
+    resolutions and switch range)."""
     from massccs_b200 import engine
     p = engine.field_params()
-    assert (p.samples, p.log2_table, p.base_res, p.finest_res) == (4000000, 18, 16, 2048)
-    assert (p.fallback_radius, p.voxel, p.err_threshold) == (3.0, 0.5, 0.05)
+    assert (p.samples, p.iterations, p.log2_table, p.base_res, p.finest_res) == (4000000, 6000, 20, 8, 128)
+    assert (p.fallback_radius, p.voxel, p.err_threshold, p.r_in, p.r_out) == (3.0, 0.5, 0.1, 6.0, 12.0)
