@@ -246,6 +246,31 @@ def cpu_baseline(json_path, config):
     return out, visits
 
 
+def cpu_baseline_batch(paths, natoms, per_ion=1000, nsample=8):
+    """The reference binary over the batched-ion workload: nsample ions spread
+    evenly over the sorted sizes, per_ion trajectories each; every ion of the
+    batch has the same trajectory count, so the batch rate is the harmonic
+    mean of the sampled ions' rates."""
+    import numpy as np
+    out = {"value": None, "unit": "trajectories/s", "cores": None, "kind": "reference", "sample": None}
+    order = np.argsort(natoms)
+    pick = [int(order[k]) for k in np.linspace(0, len(order) - 1, nsample).round().astype(int)]
+    rs = ref_setup(paths[pick[len(pick) // 2]], probe_n=200)
+    if not rs:
+        return out
+    inv, secs = [], 0.0
+    for i in pick:
+        n, t, _ = ref_sample_run(rs["binary"], paths[i], per_ion // 10, 10, rs["threads"])
+        inv.append(t / n)
+        secs += t
+    out.update(value=1.0 / float(np.mean(inv)), cores=rs["threads"], isa=rs["isa"], cpu=rs["cpu"],
+               sample=ref_describe(rs, per_ion * len(pick), per_ion // 10, 10,
+                                   f" per ion, {len(pick)} ions of {min(natoms[i] for i in pick)}-"
+                                   f"{max(natoms[i] for i in pick)} atoms spread over the sorted sizes; "
+                                   f"harmonic mean of the ions' rates; CCS time {secs:.1f} s"))
+    return out
+
+
 def fp64_check(S, eng, rnd, status, omc, m, device):
     """The metric's accuracy condition: the first m trajectories of the last
     end-to-end step rerun in the engine's FP64 mode on the same initial
@@ -345,6 +370,9 @@ def run_batch_bench(args, rank, world, local):
     ms = sum(kern) / len(kern)
     e2e_s = sum(wall) / len(wall)
     if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline_batch(paths, natoms)
         peak = E.measure_fp32_peak(local)
         fpv = FLOPS_PER_VISIT[("He", 4)]
         achieved = last["visits"] * fpv / (last["kernel_ms"] * 1e-3) / 1e12
@@ -365,7 +393,7 @@ def run_batch_bench(args, rank, world, local):
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": None,
                          "work": f"engine candidate visits x {fpv:g} flops per visit"},
-            "cpu_baseline": None,
+            "cpu_baseline": cpu,
             "gpu_launches": 3 * args.steps,
             "engine": {"lane_ms": last["lane_ms"], "warp_ms": last["warp_ms"], "parked": last["parked"],
                        "lanes_per_force": last["lanes_per_traj"]},

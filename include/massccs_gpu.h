@@ -257,11 +257,16 @@ typedef struct {
   int32_t base_res;         /* coarsest grid resolution over the domain (default 8) */
   int32_t finest_res;       /* finest grid resolution (default 128) */
   int32_t validation;       /* validation samples for the error voxels (default 1,048,576) */
-  double fallback_radius;   /* A: exact evaluation within this distance of any atom (default 3.0) */
+  double fallback_radius;   /* A: exact evaluation within this distance of any atom (default 2.0:
+                               the pair terms within r_out are always exact, so contact forces
+                               are; this zone only keeps the network off the unreachable core) */
   double voxel;             /* A: edge of the exact-evaluation bitmap's voxels (default 0.5) */
   double err_voxel;         /* A: edge of the validation-error voxels (default 2.0) */
   double err_threshold;     /* force error |G - G*| / g of a field (g: the RMS of its gradient
-                               labels) above which a voxel is evaluated exactly (default 0.1) */
+                               labels) above which a validation voxel is evaluated exactly; 0 (the
+                               default) flags none.  A probe crossing into an exact voxel sees the
+                               learned far part's error as a jump in its potential energy, which
+                               the energy test (0.5 % of the collision energy) can reject */
   double near_fraction;     /* share of samples drawn in the shell around atoms (default 0.5) */
   double near_shell;        /* A: that shell's thickness beyond fallback_radius (default 6.0) */
   double lr;                /* Adam learning rate, decayed tenfold over the run (default 1e-2) */

@@ -1148,10 +1148,10 @@ void ccs_field_params_default(ccs_field_params *p) {
   p->base_res = 8;
   p->finest_res = 128;
   p->validation = 1 << 20;
-  p->fallback_radius = 3.0;
+  p->fallback_radius = 2.0;
   p->voxel = 0.5;
   p->err_voxel = 2.0;
-  p->err_threshold = 0.1;
+  p->err_threshold = 0.0;
   p->near_fraction = 0.5;
   p->near_shell = 6.0;
   p->lr = 1e-2;
@@ -1275,8 +1275,9 @@ int ccs_field_train(ccs_ctx *c, const ccs_field_params *p, ccs_field_report *rep
     FieldK K = fs->k;
     validate_kernel<<<c->sm_count * 8, 256, 0, s>>>(K, nv, vpos, vlab, fs->nf, fs->geo,
                                                      (float)(1.0 / p->err_voxel), ev, ef, eu, verr);
-    flag_err_voxels_kernel<<<(unsigned)(((size_t)ev * ev * ev + 255) / 256), 256, 0, s>>>(
-        K, verr, ev, ratio, (float)p->err_threshold, fs->bits, cnt);
+    if (p->err_threshold > 0)  // error voxels switch to exact evaluation (0: none)
+      flag_err_voxels_kernel<<<(unsigned)(((size_t)ev * ev * ev + 255) / 256), 256, 0, s>>>(
+          K, verr, ev, ratio, (float)p->err_threshold, fs->bits, cnt);
     popcount_kernel<<<c->sm_count * 4, 256, 0, s>>>(fs->bits, fs->nwords, cnt + 1);
     std::vector<float> hf(nv), hu(nv);
     unsigned long long hc[2] = {0, 0};

@@ -98,10 +98,11 @@ def test_ctypes_layouts_match_the_headers(tmp_path):
 def test_field_params_defaults(lib):
     """The learned field's defaults: 16 levels of 2^20 rows (every level up to
     resolution 100 dense), resolutions 8..128 over the domain, 4e6 samples,
-    6000 Adam steps, the range-separation switch from 6 to 12 A, exact within
-    3 A of an atom (the measured best of the sweep over table size,
-    resolutions and switch range)."""
+    6000 Adam steps, the range-separation switch from 6 to 12 A (the measured
+    best of the sweep over table size, resolutions and switch range), exact
+    within 2 A of an atom and no error voxels (no exact/learned switching
+    where probes go)."""
     from massccs_b200 import engine
     p = engine.field_params()
     assert (p.samples, p.iterations, p.log2_table, p.base_res, p.finest_res) == (4000000, 6000, 20, 8, 128)
-    assert (p.fallback_radius, p.voxel, p.err_threshold, p.r_in, p.r_out) == (3.0, 0.5, 0.1, 6.0, 12.0)
+    assert (p.fallback_radius, p.voxel, p.err_threshold, p.r_in, p.r_out) == (2.0, 0.5, 0.0, 6.0, 12.0)
