@@ -12,6 +12,7 @@
 #include <fstream>
 #include <iostream>
 #include <sstream>
+#include <vector>
 
 #include "setup.h"
 
@@ -115,6 +116,16 @@ void MoleculeTarget::readUserFF(const std::string &path) {
 // MoleculeTarget::assignedParameter (MoleculeTarget.cpp:540-570): pair
 // parameters per gas; Lorentz-Berthelot mixing for CO2 (O and C sites) and Ar.
 void MoleculeTarget::assign(int i, const std::string &sym) {
+  if (!assign_found(i, sym)) unknown_type();
+}
+
+void MoleculeTarget::unknown_type() const {
+  throw std::invalid_argument(user_ff_flag_ ? "Atom type not found in the file user force field"
+                                            : "Atom type not found in the default data base ");
+}
+
+// the lookup itself: reads the tables only, so atoms may be assigned in parallel
+bool MoleculeTarget::assign_found(int i, const std::string &sym) {
   for (size_t k = 0; k < ff_name.size(); k++) {
     if (sym != ff_name[k]) continue;
     m[i] = ff_m[k];
@@ -130,10 +141,9 @@ void MoleculeTarget::assign(int i, const std::string &sym) {
       eps[i] = ff_eps[k];
       sig[i] = ff_sig[k];
     }
-    return;
+    return true;
   }
-  throw std::invalid_argument(user_ff_flag_ ? "Atom type not found in the file user force field"
-                                            : "Atom type not found in the default data base ");
+  return false;
 }
 
 namespace {
@@ -225,37 +235,50 @@ void MoleculeTarget::readXYZ(const std::string &path, int force_type) {
   L.next(line);  // comment
   std::vector<std::string_view> lines;
   lines.reserve((size_t)n);
-  int items0 = -1;
-  std::string_view tok[5];
-  while (L.next(line)) {
-    const int items = tokens(line, tok, 5);
-    if (items0 < 0) items0 = items;
-    else if (items != items0) throw std::invalid_argument("Error: numbers of items by lines in the xyz file");
-    lines.push_back(line);
+  while (L.next(line)) lines.push_back(line);
+  // every line must carry as many items as the first one (lines are
+  // independent: counted in parallel)
+  const long nl = (long)lines.size();
+  std::string_view tok0[5];
+  const int items0 = nl ? tokens(lines[0], tok0, 5) : -1;
+  long bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+  for (long i = 1; i < nl; i++) {
+    std::string_view tk[5];
+    bad += tokens(lines[(size_t)i], tk, 5) != items0;
   }
+  if (bad) throw std::invalid_argument("Error: numbers of items by lines in the xyz file");
   if ((int)lines.size() != n)
     throw std::invalid_argument("Error: numbers of lines and natoms are differens in the xyz file");
   const bool charges = items0 != 4;
   resize_all(*this, n);
+  // atoms are parsed in parallel (each writes only its own entries); the
+  // totals are then summed in atom order, as the reference does
+  int unknown = 0;
+#pragma omp parallel for schedule(static) reduction(+ : unknown)
   for (int i = 0; i < n; i++) {
+    std::string_view tok[5];
     std::string sym;
     double xi = 0, yi = 0, zi = 0, qi = 0;
-    const int nt = tokens(lines[i], tok, 5);
+    const int nt = tokens(lines[(size_t)i], tok, 5);
     if (nt >= 4 && plain_double(tok[1], xi) && plain_double(tok[2], yi) && plain_double(tok[3], zi) &&
         (!charges || (nt >= 5 && plain_double(tok[4], qi)))) {
       sym = std::string(tok[0]);
     } else {  // stream extraction, as the format defines it
       xi = yi = zi = qi = 0;
-      std::istringstream is{std::string(lines[i])};
+      std::istringstream is{std::string(lines[(size_t)i])};
       is >> sym >> xi >> yi >> zi;
       if (charges) is >> qi;
     }
     if (!charges || force_type == 1 || force_type == 2) qi = 0.0;
     name[i] = sym;
-    assign(i, sym);
+    unknown += !assign_found(i, sym);
     x[i] = xi; y[i] = yi; z[i] = zi; q[i] = qi;
+  }
+  if (unknown) unknown_type();
+  for (int i = 0; i < n; i++) {
     mass += m[i];
-    Q += qi;
+    Q += q[i];
   }
 }
 
@@ -272,26 +295,39 @@ void MoleculeTarget::readPQR(const std::string &path) {
   while (L.next(line))
     if (tokens(line, tok, 1) > 0 && tok[0] == "ATOM") atoms.push_back(line);
   resize_all(*this, (int)atoms.size());
+  // records parsed in parallel (each writes only its own entries); totals
+  // summed in atom order, as the reference does
+  long first_unknown = natoms, first_bad = natoms;
+#pragma omp parallel for schedule(static) reduction(min : first_unknown, first_bad)
   for (int i = 0; i < natoms; i++) {
+    std::string_view tk[9];
     std::string aname;
     long serial, chain;
-    double xi, yi, zi, qi;
-    if (tokens(atoms[i], tok, 9) >= 9 && plain_long(tok[1], serial) && plain_long(tok[4], chain) &&
-        plain_double(tok[5], xi) && plain_double(tok[6], yi) && plain_double(tok[7], zi) &&
-        plain_double(tok[8], qi)) {
-      aname = std::string(tok[2]);
+    double xi = 0, yi = 0, zi = 0, qi = 0;
+    if (tokens(atoms[(size_t)i], tk, 9) >= 9 && plain_long(tk[1], serial) && plain_long(tk[4], chain) &&
+        plain_double(tk[5], xi) && plain_double(tk[6], yi) && plain_double(tk[7], zi) &&
+        plain_double(tk[8], qi)) {
+      aname = std::string(tk[2]);
     } else {  // stream extraction, as the format defines it
-      std::istringstream is{std::string(atoms[i])};
+      std::istringstream is{std::string(atoms[(size_t)i])};
       std::string rec, res;
-      if (!(is >> rec >> serial >> aname >> res >> chain >> xi >> yi >> zi >> qi))
-        throw std::invalid_argument("Error: unsupported PQR ATOM record: " + std::string(atoms[i]));
+      if (!(is >> rec >> serial >> aname >> res >> chain >> xi >> yi >> zi >> qi)) {
+        first_bad = std::min(first_bad, (long)i);
+        continue;
+      }
     }
     const std::string sym = user_ff_flag_ ? aname : aname.substr(0, 1);
     name[i] = sym;
-    assign(i, sym);
+    if (!assign_found(i, sym)) first_unknown = std::min(first_unknown, (long)i);
     x[i] = xi; y[i] = yi; z[i] = zi; q[i] = qi;
+  }
+  // the error of the first failing record in file order, as a sequential read reports it
+  if (first_bad < first_unknown)
+    throw std::invalid_argument("Error: unsupported PQR ATOM record: " + std::string(atoms[(size_t)first_bad]));
+  if (first_unknown < natoms) unknown_type();
+  for (int i = 0; i < natoms; i++) {
     mass += m[i];
-    Q += qi;
+    Q += q[i];
   }
 }
 
@@ -303,6 +339,7 @@ void MoleculeTarget::moveToCenterOfMass() {  // MoleculeTarget.cpp:596-620
     r[2] += m[i] * z[i];
   }
   for (double &c : r) c /= mass;
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < natoms; i++) {
     x[i] -= r[0];
     y[i] -= r[1];
@@ -429,6 +466,7 @@ void MoleculeTarget::setInertia() {
     if (d > 1e-6) {
       orientateMolecule();
     } else {
+#pragma omp parallel for schedule(static)
       for (int i = 0; i < natoms; i++) {
         const double xi = x[i], yi = y[i], zi = z[i];
         x[i] = xi * vectors[0][0] + yi * vectors[0][1] + zi * vectors[0][2];

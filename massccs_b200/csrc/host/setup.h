@@ -67,6 +67,8 @@ struct MoleculeTarget {
   void readXYZ(const std::string &path, int force_type);
   void readPQR(const std::string &path);
   void assign(int i, const std::string &sym);
+  bool assign_found(int i, const std::string &sym);  // false: type not in the force field
+  [[noreturn]] void unknown_type() const;
   void moveToCenterOfMass();
   void calculateMoleculeRadius();
   void orientateMolecule();
