@@ -91,7 +91,12 @@ typedef struct {
   int32_t block_size;       /* 0 = automatic (multiple of 32) */
   uint32_t max_steps_per_try; /* 0 = 2,000,000 */
   double watchdog_s;        /* kernel wall-time budget, 0 = 600 s */
-  int32_t schedule;         /* 0 = index order, 1 = longest expected trajectories first */
+  int32_t schedule;         /* 0 = index order, 1 = longest expected trajectories first,
+                               2 = index order, and a trajectory past park_steps moves to the
+                               warp pass only once every trajectory has been taken (which ones
+                               move then depends on timing: FP32 results can differ between runs
+                               at rounding level, the two passes summing forces in different
+                               orders) */
   uint32_t park_steps;      /* steps after which a trajectory moves to the warp pass; 0 = 2048 */
   int32_t resume_block;     /* threads per trajectory in the warp pass: 32, 64 or 128; 0 = 64 */
   int32_t spec_tries;       /* failed tries after which a warp-pass trajectory runs its remaining

@@ -90,6 +90,7 @@ struct KParams {
   unsigned long long *park_next;    // next parked trajectory to resume
   unsigned long long park_cap;
   uint32_t park_steps;
+  int park_drained;                 // 1: park only once every trajectory has been taken
   int lcap;                         // warp pass: candidate-list entries (dynamic shared memory)
   // batched ions: per-ion parameters (their rnd/status/omc/steps/visits point
   // at the ion's first trajectory) and the global index of each ion's first
@@ -1561,7 +1562,9 @@ __global__ void __launch_bounds__(BLOCK, SURR ? 2 : CCS_LANE_MIN_BLOCKS)
           load_init<T, GAS>(L, lane_setup<T, GAS>(ion_params_ptr<BATCH>(kp, kpg, L.ion), L.j));
           L.mode = M_RESTART;
         }
-      } else if (kp.park && !park_full && L.nsteps >= kp.park_steps) {
+      } else if (kp.park && !park_full && L.nsteps >= kp.park_steps &&
+                 (!kp.park_drained ||
+                  ((L.nsteps & 63u) == 0 && *(volatile const unsigned long long *)kp.work >= kp.ntraj))) {
         const unsigned long long slot = atomicAdd(kp.park_count, 1ull);
         if (slot < kp.park_cap) {
           reinterpret_cast<LaneState<T> *>(kp.park)[slot] = L;

@@ -367,6 +367,7 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   k.park = c->d_park;
   k.park_cap = cap;
   k.park_steps = c->p.park_steps ? c->p.park_steps : 2048u;
+  k.park_drained = c->p.schedule == 2;
   k.park_count = c->d_work + 9;
   k.park_next = c->d_work + 10;
   rc = setup_spec(c, k, cap, s);
@@ -536,6 +537,7 @@ int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const si
   k.park = lead->d_park;
   k.park_cap = cap;
   k.park_steps = lead->p.park_steps ? lead->p.park_steps : 2048u;
+  k.park_drained = lead->p.schedule == 2;
   k.park_count = lead->d_work + 9;
   k.park_next = lead->d_work + 10;
   rc = setup_spec(lead, k, cap, s);
@@ -1258,6 +1260,7 @@ extern "C" int ccs_run_device_noalloc(ccs_ctx *c, size_t n, const double *d_rnd,
   k.park = park;
   k.park_cap = std::min<size_t>(n, std::max<size_t>(65536, n / 2));
   k.park_steps = c->p.park_steps ? c->p.park_steps : 2048u;
+  k.park_drained = c->p.schedule == 2;
   k.park_count = work + 9;
   k.park_next = work + 10;
   // everything that must start at zero: counters, statistics, park counters, error flag
