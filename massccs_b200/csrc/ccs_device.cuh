@@ -686,7 +686,10 @@ __device__ __noinline__ Acc<T, GasShape<GAS>::NS> chunked_visits(const KParams *
 // The sums are reduced per warp with a reduce-scatter butterfly and then
 // across warps in shared memory in a fixed order, so every thread ends with
 // identical bits.  All threads call this with identical arguments.
-//   sm_list: lcap ints; sm_wsum: NT/32 ints; sm_red: (NT/32 + 1) * RedShape<GAS>::P values
+//   sm_list: lcap ints; sm_wsum: NT/32 ints; sm_red: (NT/32) * RedShape<GAS>::P values, a
+//   buffer the caller alternates between consecutive calls (one barrier per
+//   call: a warp can reach the next call's barrier only after every warp has
+//   read this call's sums, so the other buffer is free when it is written)
 //   list_n, list_c: the CTA's list state (list_n < 0: no valid list)
 //   SPLIT: the near part of the range separation (candidates within r_out);
 //   the raw sums (per site f and U, then E and its gradient) go to raw[] and
@@ -783,16 +786,14 @@ __device__ __forceinline__ void eval_forces_block(const KParams &kp, const T (&p
   if constexpr (NW > 1) {
     if ((lane & ((1 << SH) - 1)) == 0) sm_red[w * P + (lane >> SH)] = v[0];
     __syncthreads();
-    if (tid < NV) {  // one thread per value sums the warps in a fixed order
-      T sum = sm_red[tid];
+    // every thread sums the warps' partials in the same fixed order
 #pragma unroll
-      for (int q = 1; q < NW; q++) sum += sm_red[q * P + tid];
-      sm_red[NW * P + tid] = sum;
+    for (int k = 0; k < NV; k++) {
+      T sum = sm_red[k];
+#pragma unroll
+      for (int q = 1; q < NW; q++) sum += sm_red[q * P + k];
+      out[k] = sum;
     }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < NV; k++) out[k] = sm_red[NW * P + k];
-    __syncthreads();
   } else {
 #pragma unroll
     for (int k = 0; k < NV; k++) out[k] = __shfl_sync(0xffffffffu, v[0], k << SH);
@@ -1608,7 +1609,8 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
   __shared__ float sm_site[NS][4 * FL_SITE_FIELDS];
   extern __shared__ int sm_list[];  // kp.lcap entries (+ LCAP with the field; dynamic shared memory)
   __shared__ int sm_wsum[NT / 32];
-  __shared__ T sm_red[(NT / 32 + 1) * RedShape<GAS>::P];
+  __shared__ T sm_red[2][(NT / 32) * RedShape<GAS>::P];  // alternating reduction buffers
+  int red = 0;
   __shared__ unsigned long long blk[8];
   __shared__ unsigned long long sm_idx;
   if (threadIdx.x < 8) blk[threadIdx.x] = 0ull;
@@ -1700,7 +1702,8 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
               // the switched exact sums over the atoms within r_out ...
               T raw[RedShape<GAS>::NV];
               eval_forces_block<T, NT, GAS, HASQ, true>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
-                                                        tid, sm_list + kp.lcap, LCAP, sm_wsum, sm_red, near_n, near_c, Kg, raw);
+                                                        tid, sm_list + kp.lcap, LCAP, sm_wsum, sm_red[red], near_n, near_c, Kg, raw);
+              red ^= 1;
               // ... plus the far parts from the network, one warp per site
               for (int s = tid >> 5; s < NS; s += NT / 32) {
                 int fl[FL_SITE_FIELDS];
@@ -1735,7 +1738,8 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
             }
           } else {
             eval_forces_block<T, NT, GAS, HASQ>(K, p, act, p[S::cs], site_offset<T, GAS>(p), fs, Us, L.nvis,
-                                                  tid, sm_list, kp.lcap, sm_wsum, sm_red, list_n, list_c, Kg);
+                                                  tid, sm_list, kp.lcap, sm_wsum, sm_red[red], list_n, list_c, Kg);
+            red ^= 1;
           }
         } else {
 #pragma unroll
