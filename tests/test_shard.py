@@ -42,6 +42,47 @@ def _worker(rank, world, port, json_path, out_dir):
         dist.destroy_process_group()
 
 
+def _host_worker(rank, world, port, json_path, out_dir):
+    """The product's host C-ABI on a rank: mh_open, mh_predraw of the whole
+    job, this rank's slice (trajectories through the oracle, no GPU here),
+    then the gather and mh_reduce."""
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        from oracle import pyoracle
+        from massccs_b200 import host, shard
+        S = host.System(json_path)
+        n = S.info["nprobe"] * S.info["niter"]
+        rnd = np.ascontiguousarray(shard.local_rnd(S.predraw(n), rank, world))
+        res = pyoracle.OracleSystem(json_path).run(rnd, nthreads=1)
+        red = shard.sharded_ccs(res["status"], res["one_minus_cos"], S.info["niter"], S.info["nprobe"],
+                                S.info["bmax"])
+        np.savez(os.path.join(out_dir, f"host{rank}.npz"), omega=red["omega"], ccs=red["ccs"], err=red["err"])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_host_api_equals_single_process(oracle, tmp_path):
+    """Ranks driving the product's host library (pre-draw and reduction in
+    C++) give the single-process CCS bit for bit (N2, uneven split)."""
+    import torch.multiprocessing as mp
+    from massccs_b200 import host
+    d = workdir()
+    p = write_input(d, input_dict("c60.xyz", "N2", 6, nprobe=25, niter=4))
+    S = host.System(p)
+    n = 100
+    full = oracle.OracleSystem(p).run(S.predraw(n), nthreads=1)
+    ref = host.reduce(4, 25, full["status"], full["one_minus_cos"], S.info["bmax"])
+    mp.start_processes(_host_worker, args=(3, _free_port(), p, str(tmp_path)), nprocs=3, join=True,
+                       start_method="spawn")
+    for r in range(3):
+        got = np.load(tmp_path / f"host{r}.npz")
+        np.testing.assert_array_equal(got["omega"], ref["omega"])
+        assert float(got["ccs"]) == ref["ccs"] and float(got["err"]) == ref["err"]
+
+
 def test_shard_range_covers_every_trajectory():
     from massccs_b200 import shard
     for n in (0, 1, 7, 300, 300001):
