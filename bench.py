@@ -246,7 +246,7 @@ def cpu_baseline(json_path, config):
     return out, visits
 
 
-def cpu_baseline_batch(paths, natoms, per_ion=1000, nsample=8):
+def cpu_baseline_batch(paths, natoms, per_ion=8000, nsample=8):
     """The reference binary over the batched-ion workload: nsample ions spread
     evenly over the sorted sizes, per_ion trajectories each; every ion of the
     batch has the same trajectory count, so the batch rate is the harmonic

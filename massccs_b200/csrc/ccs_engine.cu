@@ -230,6 +230,10 @@ KParams ccs_internal::base_params(const ccs_ctx *c) {
 
 namespace {
 
+// Park-buffer capacity of a run of n trajectories: every trajectory up to
+// 131,072, half of them beyond (a full buffer keeps the rest in their lanes)
+size_t park_capacity(size_t n) { return std::min<size_t>(n, std::max<size_t>(131072, n / 2)); }
+
 // Speculative-retry buffers for up to cap records (the park capacity) and
 // the counters d_work[11] (records) and d_work[12] (next speculative try).
 int setup_spec(ccs_ctx *c, KParams &k, size_t cap, cudaStream_t s) {
@@ -357,7 +361,7 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   // room for half the trajectories: a trajectory that finds the buffer full
   // keeps running in its lane at the lane pass's per-step cost (measured: a
   // park threshold that wanted 75,000+ slots of 75,000 tripled the run)
-  const size_t cap = std::min<size_t>(n, std::max<size_t>(65536, n / 2));
+  const size_t cap = park_capacity(n);
   if (cap * state_bytes > c->park_bytes) {
     dfree(c->d_park);
     c->park_bytes = 0;
@@ -527,7 +531,7 @@ int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const si
   k.deadline = lead->d_work + 8;
   const size_t state_bytes =
       lead->p.precision == CCS_PREC_FP64 ? sizeof(LaneState<double>) : sizeof(LaneState<float>);
-  const size_t cap = std::min<size_t>(total, std::max<size_t>(65536, total / 2));
+  const size_t cap = park_capacity(total);
   if (cap * state_bytes > lead->park_bytes) {
     dfree(lead->d_park);
     lead->park_bytes = 0;
@@ -1178,7 +1182,7 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(40) << 20;  // 40 MiB per device
 constexpr size_t NOALLOC_HEADER_BYTES = 256;                // counters, deadline and the error flag
 constexpr size_t NOALLOC_PARAMS_BYTES = 4096;               // the launch-parameter copy
 constexpr size_t NOALLOC_MAX_TRAJ = size_t(1) << 18;        // 262144 trajectories per call
-// park capacity: the rule of ccs_run_device, min(n, max(65536, n / 2)), at the largest n
+// park capacity: the rule of ccs_run_device (park_capacity) at the largest n
 constexpr size_t NOALLOC_PARK_CAP = NOALLOC_MAX_TRAJ / 2;
 static_assert(sizeof(KParams) <= NOALLOC_PARAMS_BYTES, "launch parameters do not fit");
 static_assert(NOALLOC_HEADER_BYTES + NOALLOC_PARAMS_BYTES + NOALLOC_PARK_CAP * sizeof(LaneState<double>) <=
@@ -1258,7 +1262,7 @@ extern "C" int ccs_run_device_noalloc(ccs_ctx *c, size_t n, const double *d_rnd,
   k.error = error;
   k.deadline = work + 8;
   k.park = park;
-  k.park_cap = std::min<size_t>(n, std::max<size_t>(65536, n / 2));
+  k.park_cap = park_capacity(n);
   k.park_steps = c->p.park_steps ? c->p.park_steps : 2048u;
   k.park_drained = c->p.schedule == 2;
   k.park_count = work + 9;
