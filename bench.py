@@ -631,6 +631,10 @@ def main():
     L = E.load_library()
     HL = H.load_library()
 
+    # the reduction's iterations x probes must cover exactly the job's
+    # trajectories (a job smaller than the workload's, e.g. --ntraj, too)
+    it_n = S.info["niter"] if job % S.info["niter"] == 0 else 1
+
     def step_e2e():
         HL.mh_predraw(S._h, seed, job, pin_np.ctypes.data_as(ctypes.c_void_p))
         stt = E.CcsStats()
@@ -642,10 +646,9 @@ def main():
             dist.all_gather_into_tensor(g_st, torch.from_numpy(st_pin).to(dev))
             dist.all_gather_into_tensor(g_om, torch.from_numpy(om_pin).to(dev))
             if rank == 0:
-                H.reduce(S.info["niter"] * world, S.info["nprobe"], g_st.cpu().numpy(), g_om.cpu().numpy(),
-                         S.info["bmax"])
+                H.reduce(it_n, job // it_n, g_st.cpu().numpy(), g_om.cpu().numpy(), S.info["bmax"])
         else:
-            H.reduce(S.info["niter"], S.info["nprobe"], st_pin, om_pin, S.info["bmax"])
+            H.reduce(it_n, job // it_n, st_pin, om_pin, S.info["bmax"])
 
     step_e2e()
     barrier()

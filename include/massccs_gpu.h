@@ -96,9 +96,7 @@ typedef struct {
                                warp pass only once every trajectory has been taken (which ones
                                move then depends on timing: FP32 results can differ between runs
                                at rounding level, the two passes summing forces in different
-                               orders), 3 = index order, and the trajectories taken in the
-                               queue's last lane-load park after park_steps / 4 steps (a pure
-                               function of the queue position: reproducible) */
+                               orders) */
   uint32_t park_steps;      /* steps after which a trajectory moves to the warp pass; 0 = 2048 */
   int32_t resume_block;     /* threads per trajectory in the warp pass: 32, 64 or 128; 0 = 64 */
   int32_t spec_tries;       /* failed tries after which a warp-pass trajectory runs its remaining

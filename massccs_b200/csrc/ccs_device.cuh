@@ -91,8 +91,6 @@ struct KParams {
   unsigned long long park_cap;
   uint32_t park_steps;
   int park_drained;                 // 1: park only once every trajectory has been taken
-  unsigned long long park_late_from;  // trajectories taken from this queue position on park after
-  uint32_t park_steps_late;           // park_steps_late steps (the last lane-load of the queue)
   int lcap;                         // warp pass: candidate-list entries (dynamic shared memory)
   // batched ions: per-ion parameters (their rnd/status/omc/steps/visits point
   // at the ion's first trajectory) and the global index of each ion's first
@@ -1320,8 +1318,7 @@ __global__ void __launch_bounds__(BLOCK, SURR ? 2 : CCS_LANE_MIN_BLOCKS)
   L.mode = M_IDLE;
   L.ion = 0;
   const unsigned long long deadline = *(volatile const unsigned long long *)kp.deadline;
-  bool park_full = false;
-  uint32_t park_at = kp.park_steps;  // this lane's threshold (set with each trajectory taken)  // the park buffer filled up: stop asking for slots (it only fills)
+  bool park_full = false;  // the park buffer filled up: stop asking for slots (it only fills)
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   uint32_t tmem = 0, tc_phase = 0;
   if constexpr (SURR) tmem = tc_setup(kp.field, tc_smem);
@@ -1331,7 +1328,6 @@ __global__ void __launch_bounds__(BLOCK, SURR ? 2 : CCS_LANE_MIN_BLOCKS)
     for (;;) {
       const unsigned long long jj = atomicAdd(kp.work, 1ull);
       if (jj >= kp.ntraj || *(volatile int *)kp.error) { L.mode = M_IDLE; return; }
-      park_at = jj >= kp.park_late_from ? kp.park_steps_late : kp.park_steps;
       if constexpr (BATCH) {  // the ion holding global trajectory jj (bisection of the ion starts)
         int lo = 0, hi = kp.nions;
         while (hi - lo > 1) {
@@ -1567,7 +1563,7 @@ __global__ void __launch_bounds__(BLOCK, SURR ? 2 : CCS_LANE_MIN_BLOCKS)
           load_init<T, GAS>(L, lane_setup<T, GAS>(ion_params_ptr<BATCH>(kp, kpg, L.ion), L.j));
           L.mode = M_RESTART;
         }
-      } else if (kp.park && !park_full && L.nsteps >= park_at &&
+      } else if (kp.park && !park_full && L.nsteps >= kp.park_steps &&
                  (!kp.park_drained ||
                   ((L.nsteps & 63u) == 0 && *(volatile const unsigned long long *)kp.work >= kp.ntraj))) {
         const unsigned long long slot = atomicAdd(kp.park_count, 1ull);

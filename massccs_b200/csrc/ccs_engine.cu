@@ -168,7 +168,6 @@ KParams ccs_internal::base_params(const ccs_ctx *c) {
   for (int d = 0; d < 3; d++) { k.bb_lo[d] = c->bb_lo[d]; k.bb_hi[d] = c->bb_hi[d]; }
   k.reach = c->reach;
   k.lcap = c->lcap;
-  k.park_late_from = ~0ull;  // one park threshold unless a schedule sets a late one
   k.allpairs = c->allpairs;
   k.coul_on = c->coul_on;
   k.dip_on = c->dip_on;
@@ -230,19 +229,6 @@ KParams ccs_internal::base_params(const ccs_ctx *c) {
 }
 
 namespace {
-
-// schedule 3: the trajectories taken in the queue's last lane-load (grid x
-// block positions) park after a quarter of park_steps, so the lane pass ends
-// with fewer lanes still running; a pure function of the queue position, so
-// results do not depend on timing.  Other schedules: one threshold.
-void set_late_parking(const ccs_params &p, KParams &k, size_t n, size_t lanes) {
-  k.park_late_from = ~0ull;
-  k.park_steps_late = k.park_steps;
-  if (p.schedule == 3) {
-    k.park_late_from = n > lanes ? (unsigned long long)(n - lanes) : 0ull;
-    k.park_steps_late = std::max(1u, k.park_steps / 4);
-  }
-}
 
 // Park-buffer capacity of a run of n trajectories: every trajectory up to
 // 131,072, half of them beyond (a full buffer keeps the rest in their lanes)
@@ -386,7 +372,6 @@ int run_device(ccs_ctx *c, size_t n, const double *d_rnd, size_t stride, int8_t 
   k.park_cap = cap;
   k.park_steps = c->p.park_steps ? c->p.park_steps : 2048u;
   k.park_drained = c->p.schedule == 2;
-  set_late_parking(c->p, k, n, grid * (size_t)block);
   k.park_count = c->d_work + 9;
   k.park_next = c->d_work + 10;
   rc = setup_spec(c, k, cap, s);
@@ -557,8 +542,6 @@ int run_batch_device(ccs_ctx *lead, ccs_ctx *const *ions, size_t nions, const si
   k.park_cap = cap;
   k.park_steps = lead->p.park_steps ? lead->p.park_steps : 2048u;
   k.park_drained = lead->p.schedule == 2;
-  k.park_late_from = ~0ull;
-  k.park_steps_late = k.park_steps;
   k.park_count = lead->d_work + 9;
   k.park_next = lead->d_work + 10;
   rc = setup_spec(lead, k, cap, s);
@@ -1295,7 +1278,6 @@ extern "C" int ccs_run_device_noalloc(ccs_ctx *c, size_t n, const double *d_rnd,
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn, block, 0));
   size_t grid = (size_t)std::max(per_sm, 1) * c->sm_count;
   grid = std::min(grid, std::max<size_t>(1, (n + block - 1) / block));
-  set_late_parking(c->p, k, n, grid * (size_t)block);
   CK(cudaEventRecord(c->ev[2], s));
   CK(cudaEventRecord(c->ev[5], s));
   fn<<<(unsigned)grid, block, 0, s>>>(k, kparams);
