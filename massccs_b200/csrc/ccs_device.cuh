@@ -133,7 +133,23 @@ struct SpecRec {
   unsigned long long j;
   uint32_t ion, nsteps, nvis; // steps and visits of the tries before
   int tries, maxTries;
+  int ready;                  // set (after a fence) once the fields above are written
 };
+
+// A record's fields as its writer published them: read past L1 (a record
+// is written by another CTA during the same launch).
+__device__ __forceinline__ SpecRec load_spec_rec(const SpecRec *p) {
+  SpecRec R;
+  R.Ei = __ldcg(&p->Ei);
+  R.j = __ldcg(&p->j);
+  R.ion = __ldcg(&p->ion);
+  R.nsteps = __ldcg(&p->nsteps);
+  R.nvis = __ldcg(&p->nvis);
+  R.tries = __ldcg(&p->tries);
+  R.maxTries = __ldcg(&p->maxTries);
+  R.ready = 1;
+  return R;
+}
 // The end of one speculative try: 1 scatter (omc valid), 3 capped or watchdog,
 // 4 failed the angle test, 5 failed the energy test.
 struct SpecOut {
@@ -1616,10 +1632,10 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
   if (threadIdx.x < 8) blk[threadIdx.x] = 0ull;
   __syncthreads();
   const int tid = threadIdx.x;
-  const bool spec = kp.spec_phase != 0;
+  const bool spec_launch = kp.spec_phase != 0;
   const unsigned long long deadline = *(volatile const unsigned long long *)kp.deadline;
   unsigned long long np;
-  if (spec) {
+  if (spec_launch) {
     np = *(volatile unsigned long long *)kp.spec_count;
     if (np > kp.spec_cap) np = kp.spec_cap;
     np *= SPEC_SLOTS;
@@ -1627,23 +1643,55 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
     np = *(volatile unsigned long long *)kp.park_count;
     if (np > kp.park_cap) np = kp.park_cap;
   }
-  unsigned long long *next = spec ? kp.spec_next : kp.park_next;
+  unsigned long long *next = spec_launch ? kp.spec_next : kp.park_next;
   // speculation pays when the warp pass is bound by its longest chains of
   // tries, not while parked trajectories wait for a CTA (then the extra
   // tries only add work): a failed try is handed over when few trajectories
   // were parked at all, or once every parked trajectory has been taken
-  const bool may_spec = kp.spec_rec && !spec;
+  const bool may_spec = kp.spec_rec && !spec_launch;
+  // phase 0 CTAs that find the park queue drained go on with the speculative
+  // tries recorded so far (claimed without waiting: a try whose record is not
+  // yet published, and every later one, is left to the phase-1 launch)
+  bool park_done = spec_launch;
+  __shared__ int sm_kind;
   for (;;) {
-    if (tid == 0) sm_idx = *(volatile int *)kp.error ? np : atomicAdd(next, 1ull);
+    if (tid == 0) {
+      unsigned long long v = ~0ull;
+      int kind = spec_launch ? 1 : 0;
+      if (!*(volatile int *)kp.error) {
+        if (!park_done) {
+          v = atomicAdd(next, 1ull);
+          if (v >= np) { v = ~0ull; park_done = true; }
+        } else if (spec_launch) {
+          v = atomicAdd(next, 1ull);
+          if (v >= np) v = ~0ull;
+        }
+        if (v == ~0ull && may_spec) {
+          kind = 1;
+          for (int t = 0; t < 32; t++) {  // bounded compare-and-swap claim
+            unsigned long long cnt = *(volatile unsigned long long *)kp.spec_count;
+            if (cnt > kp.spec_cap) cnt = kp.spec_cap;
+            const unsigned long long cur = *(volatile unsigned long long *)kp.spec_next;
+            if (cur >= cnt * SPEC_SLOTS) break;
+            if (!*(volatile int *)&kp.spec_rec[cur / SPEC_SLOTS].ready) break;
+            if (atomicCAS(kp.spec_next, cur, cur + 1) == cur) { v = cur; break; }
+          }
+          __threadfence();  // the record's fields after its ready flag
+        }
+      }
+      sm_idx = v;
+      sm_kind = kind;
+    }
     __syncthreads();
     const unsigned long long idx = sm_idx;
+    const bool spec = sm_kind != 0;  // this item is a speculative try
     __syncthreads();
-    if (idx >= np) break;
+    if (idx == ~0ull) break;
     LaneState<T> L;
     unsigned long long rec = 0;
     if (spec) {  // try k of record rec, from the trajectory's initial state
       rec = idx / SPEC_SLOTS;
-      const SpecRec R = kp.spec_rec[rec];
+      const SpecRec R = load_spec_rec(kp.spec_rec + rec);
       const int k = R.tries + (int)(idx % SPEC_SLOTS);
       if (k > 8) continue;  // beyond the reference's last try (block-uniform)
       L.j = R.j;
@@ -1781,7 +1829,7 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
         if (tid == 0) write_result(K, L, 2, 0.0, blk);
         break;
       }
-      if (may_spec && L.tries >= kp.spec_from) {  // hand the remaining tries to the speculative phase
+      if (may_spec && !spec && L.tries >= kp.spec_from) {  // hand the remaining tries to the speculative phase
         if (tid == 0) {
           const bool drained = np <= kp.spec_max_parked || *(volatile unsigned long long *)kp.park_next >= np;
           const unsigned long long slot = drained ? atomicAdd(kp.spec_count, 1ull) : ~0ull;
@@ -1795,7 +1843,10 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
             R.nvis = L.nvis;
             R.tries = L.tries;
             R.maxTries = L.maxTries;
+            R.ready = 0;
             kp.spec_rec[slot] = R;
+            __threadfence();  // the fields before the flag that publishes them
+            *(volatile int *)&kp.spec_rec[slot].ready = 1;
           }
         }
         __syncthreads();

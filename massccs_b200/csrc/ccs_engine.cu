@@ -256,6 +256,8 @@ int setup_spec(ccs_ctx *c, KParams &k, size_t cap, cudaStream_t s) {
   k.spec_from = std::max(SPEC_FROM_MIN, c->p.spec_tries > 0 ? c->p.spec_tries : 2);
   if (c->p.spec_tries < 0) k.spec_rec = nullptr;  // speculation off
   CK(cudaMemsetAsync(c->d_work + 11, 0, 2 * sizeof(unsigned long long), s));
+  // every record unpublished (phase-0 CTAs claim only published records' tries)
+  if (k.spec_rec) CK(cudaMemsetAsync(c->d_spec_rec, 0, cap * sizeof(SpecRec), s));
   return CCS_OK;
 }
 

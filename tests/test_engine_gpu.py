@@ -76,7 +76,8 @@ def test_site_forces_match_oracle(oracle, target, gas, ft, prec):
             assert reach.sum() > 100
             # all-pairs types sum every atom's unshifted Coulomb term: FP32 rounding
             # scales with the sum of their magnitudes (64 units of 2^-24 of it)
-            floor = 2e-4 + (64 * 2.0 ** -24 * _coulomb_abs_sum(s, site, pts) if ft in (1, 3, 5) else 0.0)
+            floor = 2e-4 + (64 * 2.0 ** -24 * _coulomb_abs_sum(s, site, pts) if ft in (1, 3, 5)
+                            else np.zeros(len(pts)))
             assert np.all(fn[reach] <= 1e-4 * np.linalg.norm(fo[reach], axis=1) + 1e-4), (site, fn[reach].max())
             assert np.all(np.abs(U - Uo)[reach] <= 1e-5 * np.abs(Uo[reach]) + floor[reach]), \
                 (site, (np.abs(U - Uo) - 1e-5 * np.abs(Uo) - floor)[reach].max())

@@ -88,12 +88,15 @@ def test_noalloc_matches_run_device_twice(tmp_path, kind, park, precision):
 
 
 def test_noalloc_parks_beyond_65536(tmp_path):
-    """150,000 trajectories with a 16-step park threshold: more than 65,536
-    park, so the park region of the array is used at the capacity
-    ccs_run_device gives that size (n / 2), and the results stay identical."""
+    """131,072 trajectories with a 16-step park threshold: almost all park
+    (more than 65,536), so the park region of the array is used at the
+    capacity ccs_run_device gives that size (every trajectory), and the
+    results stay identical.  (A run whose trajectories outnumber the park
+    slots keeps the excess in the lane pass, and which ones find the buffer
+    full depends on timing, so such runs agree only to FP32 rounding.)"""
     import torch
-    S = _system("c60_he", str(tmp_path), nprobe=150000)
-    n = 150000
+    S = _system("c60_he", str(tmp_path), nprobe=131072)
+    n = 131072
     eng = S.engine(precision=0, lanes_per_traj=32, park_steps=16)
     dev = torch.device("cuda", 0)
     stream = torch.cuda.Stream(dev)
