@@ -105,6 +105,7 @@ struct KParams {
   struct SpecRec *spec_rec;
   struct SpecOut *spec_out;
   unsigned long long *spec_count, *spec_next;
+  unsigned long long *park_active;  // parked trajectories taken and not yet finished or recorded
   unsigned long long spec_cap;
   int spec_phase;
   int spec_from;  // failed tries after which a warp-pass trajectory is handed over
@@ -1649,9 +1650,11 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
   // tries only add work): a failed try is handed over when few trajectories
   // were parked at all, or once every parked trajectory has been taken
   const bool may_spec = kp.spec_rec && !spec_launch;
-  // phase 0 CTAs that find the park queue drained go on with the speculative
-  // tries recorded so far (claimed without waiting: a try whose record is not
-  // yet published, and every later one, is left to the phase-1 launch)
+  // Phase-0 CTAs that find the park queue drained stay and run the
+  // speculative tries as their records are published, until no parked
+  // trajectory is still running (then every record is final); the phase-1
+  // launch runs whatever is left (records beyond this, or after a timeout).
+  // The wait polls with a sleep and ends at the watchdog's deadline.
   bool park_done = spec_launch;
   __shared__ int sm_kind;
   for (;;) {
@@ -1660,21 +1663,40 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
       int kind = spec_launch ? 1 : 0;
       if (!*(volatile int *)kp.error) {
         if (!park_done) {
+          if (may_spec) atomicAdd(kp.park_active, 1ull);  // before taking: a poller never misses it
           v = atomicAdd(next, 1ull);
-          if (v >= np) { v = ~0ull; park_done = true; }
+          if (v >= np) {
+            v = ~0ull;
+            park_done = true;
+            if (may_spec) atomicAdd(kp.park_active, ~0ull);  // minus one
+          }
         } else if (spec_launch) {
           v = atomicAdd(next, 1ull);
           if (v >= np) v = ~0ull;
         }
         if (v == ~0ull && may_spec) {
           kind = 1;
-          for (int t = 0; t < 32; t++) {  // bounded compare-and-swap claim
+          for (unsigned poll = 0; poll < (1u << 26); poll++) {
+            if ((poll & 255u) == 255u && (global_ns() > deadline || *(volatile int *)kp.error)) {
+              atomicExch(kp.error, 1);  // the watchdog: stop waiting
+              break;
+            }
+            // the running count first: once it is zero every record is published
+            const unsigned long long active = *(volatile unsigned long long *)kp.park_active;
+            __threadfence();
             unsigned long long cnt = *(volatile unsigned long long *)kp.spec_count;
             if (cnt > kp.spec_cap) cnt = kp.spec_cap;
             const unsigned long long cur = *(volatile unsigned long long *)kp.spec_next;
-            if (cur >= cnt * SPEC_SLOTS) break;
-            if (!*(volatile int *)&kp.spec_rec[cur / SPEC_SLOTS].ready) break;
-            if (atomicCAS(kp.spec_next, cur, cur + 1) == cur) { v = cur; break; }
+            if (cur < cnt * SPEC_SLOTS) {
+              if (*(volatile int *)&kp.spec_rec[cur / SPEC_SLOTS].ready &&
+                  atomicCAS(kp.spec_next, cur, cur + 1) == cur) {
+                v = cur;
+                break;
+              }
+              continue;  // being published, or another CTA took it: look again
+            }
+            if (active == 0) break;  // nothing left to come
+            __nanosleep(2000);
           }
           __threadfence();  // the record's fields after its ready flag
         }
@@ -1810,7 +1832,7 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
           o.nvis = L.nvis;
           o.code = r == S_SCATTER ? 1 : r == S_CAPPED ? 3 : r == S_RETRY_ANGLE ? 4 : 5;
           o.pad = 0;
-          kp.spec_out[rec * SPEC_SLOTS + (L.tries - kp.spec_rec[rec].tries)] = o;
+          kp.spec_out[rec * SPEC_SLOTS + (L.tries - __ldcg(&kp.spec_rec[rec].tries))] = o;
         }
         break;
       }
@@ -1858,6 +1880,11 @@ __global__ void __launch_bounds__(NT, CCS_WARP_MIN_BLOCKS(T, NT, GAS)) resume_ke
       L.mode = M_RESTART;
       list_n = -1;
       near_n = -1;
+    }
+    // a parked trajectory has ended (or its record is published): one fewer running
+    if (tid == 0 && !spec && may_spec) {
+      __threadfence();
+      atomicAdd(kp.park_active, ~0ull);
     }
     __syncthreads();
   }

@@ -235,7 +235,8 @@ namespace {
 size_t park_capacity(size_t n) { return std::min<size_t>(n, std::max<size_t>(131072, n / 2)); }
 
 // Speculative-retry buffers for up to cap records (the park capacity) and
-// the counters d_work[11] (records) and d_work[12] (next speculative try).
+// the counters d_work[11] (records), d_work[12] (next speculative try) and
+// d_work[13] (parked trajectories still running).
 int setup_spec(ccs_ctx *c, KParams &k, size_t cap, cudaStream_t s) {
   // records come only from warp passes with at most 2 parked trajectories per
   // CTA slot (a few thousand); an overflow falls back to tries in sequence
@@ -251,11 +252,12 @@ int setup_spec(ccs_ctx *c, KParams &k, size_t cap, cudaStream_t s) {
   k.spec_out = c->d_spec_out;
   k.spec_count = c->d_work + 11;
   k.spec_next = c->d_work + 12;
+  k.park_active = c->d_work + 13;
   k.spec_cap = cap;
   k.spec_phase = 0;
   k.spec_from = std::max(SPEC_FROM_MIN, c->p.spec_tries > 0 ? c->p.spec_tries : 2);
   if (c->p.spec_tries < 0) k.spec_rec = nullptr;  // speculation off
-  CK(cudaMemsetAsync(c->d_work + 11, 0, 2 * sizeof(unsigned long long), s));
+  CK(cudaMemsetAsync(c->d_work + 11, 0, 3 * sizeof(unsigned long long), s));
   // every record unpublished (phase-0 CTAs claim only published records' tries)
   if (k.spec_rec) CK(cudaMemsetAsync(c->d_spec_rec, 0, cap * sizeof(SpecRec), s));
   return CCS_OK;
@@ -656,7 +658,7 @@ int ccs_create(ccs_ctx **out, int device) {
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(CCS_ERR_CUDA);
   for (auto &e : c->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return bail(CCS_ERR_CUDA);
-  if (cudaMalloc(&c->d_work, 13 * sizeof(unsigned long long)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
+  if (cudaMalloc(&c->d_work, 14 * sizeof(unsigned long long)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
   if (cudaMalloc(&c->d_error, sizeof(int)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
   if (cudaMalloc(&c->d_kparams, sizeof(KParams)) != cudaSuccess) return bail(CCS_ERR_NOMEM);
   *out = c;
