@@ -98,7 +98,9 @@ typedef struct {
                                at rounding level, the two passes summing forces in different
                                orders) */
   uint32_t park_steps;      /* steps after which a trajectory moves to the warp pass; 0 = 2048 */
-  int32_t resume_block;     /* threads per trajectory in the warp pass: 32, 64 or 128; 0 = 64 */
+  int32_t resume_block;     /* threads per trajectory in the warp pass: 32, 64 or 128; 0 = 32 for
+                               N2/CO2 in FP32 on targets whose candidate lists fit 2048 entries,
+                               else 64 */
   int32_t spec_tries;       /* failed tries after which a warp-pass trajectory runs its remaining
                                tries at once (2..8); 0 = default, < 0 = never */
 } ccs_params;
