@@ -394,7 +394,8 @@ def run_batch_bench(args, rank, world, local):
                          "frac": achieved / peak if peak else None, "traffic": None,
                          "work": f"engine candidate visits x {fpv:g} flops per visit"},
             "cpu_baseline": cpu,
-            "gpu_launches": 3 * args.steps,
+            # per run: watchdog arm, lane pass, warp pass (two launches), verdicts of the speculative tries
+            "gpu_launches": 5 * args.steps,
             "engine": {"lane_ms": last["lane_ms"], "warp_ms": last["warp_ms"], "parked": last["parked"],
                        "lanes_per_force": last["lanes_per_traj"]},
             "clocks": clocks.summary(),
@@ -506,7 +507,9 @@ def run_field_bench(args, rank, world, local):
                     "h2d_bytes_per_step": 9 * 8 * n, "d2h_bytes_per_step": 9 * n,
                     "includes": "ccs_run with the learned field (H2D, both passes, D2H) and the reduction; "
                                 "training excluded (set-up, in `training`)"},
-            "accuracy": acc, "cpu_baseline": cpu, "gpu_launches": 6 * args.steps,
+            # per step two runs (plain and field) of 5 kernels each: watchdog arm, lane pass,
+            # warp pass (two launches), verdicts of the speculative tries
+            "accuracy": acc, "cpu_baseline": cpu, "gpu_launches": 10 * args.steps,
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -709,7 +712,8 @@ def main():
                          "frac_executed": (n * engine_visits * fpv / kernel_s / 1e12) / peak if peak else None},
             "cpu_baseline": cpu,
             "accuracy": accuracy,
-            "gpu_launches": 3 * args.steps,
+            # per run: watchdog arm, lane pass, warp pass (two launches), verdicts of the speculative tries
+            "gpu_launches": 5 * args.steps,
             "engine": {"lane_ms": last["lane_ms"], "warp_ms": last["warp_ms"], "parked": last["parked"],
                        "lanes_per_force": last["lanes_per_traj"], "scatter_fraction": nscatter / n,
                        "steps_per_traj": last["steps"] / n},
