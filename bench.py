@@ -1,12 +1,15 @@
 """Benchmark of the trajectory-method CCS hot path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config globule_n2|c60_he]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME]
     python bench.py --impl reference ...   # the reference's own CPU implementation
 
 One step = one pass of the trajectory loop over the workload's trajectories:
-the charged 1231-atom globule with the 3-site N2 probe, 3e5 trajectories (the
-configuration the headline metric is quoted on; `--config c60_he` runs the
-60-atom cage with He).  Prints one JSON line.
+by default the charged 1231-atom globule with the 3-site N2 probe, 3e5
+trajectories (the configuration the headline metric is quoted on).  Other
+workloads (`--config`): c60_he (60-atom cage, He), shell_he / shell_n2 (5e5-atom
+shell), batch_he (256 ions in one batched call), field_n2 / field_co2
+(20,000-atom globule, plain FP32 and the learned field side by side).  Prints
+one JSON line.
 
 value      trajectories/s with the random inputs resident in HBM (ccs_run_device),
            whole job over all ranks (each rank its own trajectories: weak scaling)
