@@ -175,6 +175,17 @@ def test_equipotential_ellipsoid_matches_reference_binary(host, target, gas, ft)
     assert S.info["bmax"] == max(S.info["a"], S.info["b"], S.info["c"])
 
 
+def test_setup_device_key(host):
+    """input.json's "setup_device" extension key: cpu, gpu or auto (the CPU
+    path needs no GPU; anything else is an input error)."""
+    d = workdir()
+    cfg = dict(input_dict("c60.xyz"), Equipotential="yes", setup_device="cpu")
+    S = host.System(write_input(d, cfg, name="a.json"))
+    assert S.info["bmax"] > 0
+    with pytest.raises(Exception, match="setup_device"):
+        host.System(write_input(d, dict(input_dict("c60.xyz"), setup_device="tpu"), name="b.json"))
+
+
 def test_devices_key(host):
     """input.json's "devices" extension key: a count (GPUs 0..N-1) or a list."""
     d = workdir()
